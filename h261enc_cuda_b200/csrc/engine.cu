@@ -1,0 +1,692 @@
+/*
+ * engine.cu -- the batched encode engine behind include/h261b.h.
+ *
+ * Memory: every open session owns two reconstruction pictures in HBM (they
+ * alternate as reference and output) and its denoise state, taken from a
+ * size-class slab pool so that opening a session in steady state does not
+ * call cudaMalloc.  Queued source pictures are packed by h261b_session_submit
+ * into a pinned upload arena; a step moves the whole arena with one copy,
+ * runs one launch over the flat (session, MB) work list, and brings the
+ * compact results of all sessions back with one copy.  Arenas, descriptors
+ * and results are double-buffered by step parity, so the host can queue the
+ * next step and read the previous results while a step runs.
+ *
+ * Tuning: when warps_per_cta is 0 the first steps try each launch shape on
+ * live work (the results do not depend on it) and keep the fastest by CUDA
+ * event time.
+ */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.h"
+#include "h261b_device.h"
+
+namespace h261b {
+
+static thread_local char g_err[512];
+
+void set_error(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+void clear_error() { g_err[0] = 0; }
+
+/* ---------------------------------------------------------------- pool */
+
+/* slabs of equal-size device blocks, one slab list per block size */
+class DevicePool {
+  public:
+    ~DevicePool()
+    {
+        for (void *p : slabs_)
+            cudaFree(p);
+    }
+    int get(size_t bytes, void **out)
+    {
+        bytes = align_up(bytes, 256);
+        auto &fl = free_[bytes];
+        if (fl.empty()) {
+            const size_t per = std::max<size_t>(1, (size_t)(64u << 20) / bytes);
+            void *slab = nullptr;
+            cudaError_t err = cudaMalloc(&slab, per * bytes);
+            if (err != cudaSuccess) {
+                set_error("device pool: cudaMalloc(%zu) failed: %s", per * bytes, cudaGetErrorString(err));
+                return H261B_ERR_NOMEM;
+            }
+            slabs_.push_back(slab);
+            held_ += per * bytes;
+            for (size_t i = 0; i < per; i++)
+                fl.push_back((char *)slab + i * bytes);
+        }
+        *out = fl.back();
+        fl.pop_back();
+        return H261B_OK;
+    }
+    void put(size_t bytes, void *p) { free_[align_up(bytes, 256)].push_back(p); }
+    int64_t held() const { return (int64_t)held_; }
+
+  private:
+    std::map<size_t, std::vector<void *>> free_;
+    std::vector<void *> slabs_;
+    size_t held_ = 0;
+};
+
+/* pinned host + device buffer pair of one capacity */
+struct Mirror {
+    uint8_t *host = nullptr;
+    uint8_t *dev = nullptr;
+    size_t cap = 0;
+    /* grow to at least `bytes`; the first `keep` host bytes survive */
+    int reserve(size_t bytes, size_t keep = 0)
+    {
+        if (bytes <= cap)
+            return H261B_OK;
+        size_t c = align_up(std::max<size_t>(bytes, 1 << 16) * 5 / 4, 4096);
+        uint8_t *nh = nullptr, *nd = nullptr;
+        cudaError_t e1 = cudaMallocHost(&nh, c);
+        cudaError_t e2 = cudaMalloc(&nd, c);
+        if (e1 != cudaSuccess || e2 != cudaSuccess) {
+            set_error("arena allocation of %zu bytes failed", c);
+            if (nh)
+                cudaFreeHost(nh);
+            if (nd)
+                cudaFree(nd);
+            return H261B_ERR_NOMEM;
+        }
+        if (keep && host)
+            memcpy(nh, host, std::min(keep, cap));
+        release();
+        host = nh;
+        dev = nd;
+        cap = c;
+        return H261B_OK;
+    }
+    void release()
+    {
+        if (host)
+            cudaFreeHost(host);
+        if (dev)
+            cudaFree(dev);
+        host = dev = nullptr;
+        cap = 0;
+    }
+};
+
+struct Session {
+    bool open = false;
+    int32_t w = 0, h = 0, mbw = 0, mbh = 0, nmb = 0;
+    int32_t quant = 8, intra_period = 0;
+    int32_t frame_index = 0;       /* next picture number                 */
+    PictureLayout lay;
+    uint8_t *rec[2] = { nullptr, nullptr };
+    int rec_cur = 0;               /* holds the latest reconstruction     */
+    h261b_denoise_dev_t *dn = nullptr;
+    size_t slot_bytes = 0;
+    /* queued picture: in the upload arena, or already in device memory */
+    bool queued = false;
+    size_t src_off = 0;
+    const uint8_t *dev_src[3] = { nullptr, nullptr, nullptr };
+    int32_t queued_quant = 0;
+    /* last completed step */
+    bool has_result = false;
+    int res_parity = 0;
+    size_t info_off = 0, level_off = 0;
+    int32_t res_frame = 0, res_type = 0, res_quant = 0;
+};
+
+} // namespace h261b
+
+using namespace h261b;
+
+struct h261b_engine_s {
+    h261b_engine_config_t cfg;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    DevicePool pool;
+    std::vector<Session> sessions;
+    int32_t open_count = 0;
+    int64_t session_bytes = 0;
+
+    Mirror upload[2];          /* queued source pictures                  */
+    Mirror results[2];         /* mb info + levels of every session        */
+    Mirror desc[2];            /* session descriptors + work list           */
+    size_t upload_used = 0;    /* bytes queued into upload[parity]         */
+    int parity = 0;            /* arena the next step uses                 */
+    cudaEvent_t h2d_done[2] = { nullptr, nullptr };
+    cudaEvent_t step_done[2] = { nullptr, nullptr };
+    cudaEvent_t k_start = nullptr, k_end = nullptr;
+    bool upload_checked = false;
+    bool in_flight[2] = { false, false };
+    int last_parity = -1;
+    std::vector<int32_t> last_stepped;
+
+    /* launch tuning */
+    int warps = 4, ctas = 0;
+    std::vector<std::pair<int, int>> tune_cands;
+    std::vector<float> tune_ms;
+    size_t tune_next = 0;
+    bool tuned = false;
+};
+
+static const char *k_version = "h261b 0.1 (sm_100a)";
+
+extern "C" const char *h261b_last_error(void) { return g_err; }
+extern "C" const char *h261b_version(void) { return k_version; }
+
+extern "C" void h261b_engine_config_default(h261b_engine_config_t *c)
+{
+    memset(c, 0, sizeof(*c));
+    c->device = 0;
+    c->max_sessions = 4096;
+    c->hbm_budget_bytes = 0;
+    c->me_mode = H261B_ME_REFERENCE;
+    c->fmad = 1;
+    c->warps_per_cta = 0;
+    c->max_ctas = 0;
+    c->use_graphs = 0;
+}
+
+extern "C" int64_t h261b_session_bytes(int32_t w, int32_t h)
+{
+    if (w < 16 || h < 16 || (w & 15) || (h & 15))
+        return -1;
+    return (int64_t)(2 * PictureLayout::of(w, h).bytes + align_up(sizeof(h261b_denoise_dev_t), 256));
+}
+
+extern "C" int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engine_t **out)
+{
+    clear_error();
+    if (!cfg || !out || cfg->max_sessions < 1 || cfg->max_sessions > 65536 || cfg->warps_per_cta < 0 ||
+        cfg->warps_per_cta > 8 || (cfg->me_mode != 0 && cfg->me_mode != 1)) {
+        set_error("h261b_engine_create: bad configuration");
+        return H261B_ERR_ARG;
+    }
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || cfg->device < 0 || cfg->device >= ndev) {
+        set_error("h261b_engine_create: CUDA device %d not available", cfg->device);
+        return H261B_ERR_NO_DEVICE;
+    }
+    H261B_CUDA_TRY(cudaSetDevice(cfg->device));
+    h261b_engine_t *e = new h261b_engine_s();
+    e->cfg = *cfg;
+    e->sessions.resize((size_t)cfg->max_sessions);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess || h261b_set_quant_table() != 0 ||
+        cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        set_error("h261b_engine_create: device setup failed: %s", cudaGetErrorString(cudaGetLastError()));
+        delete e;
+        return H261B_ERR_CUDA;
+    }
+    e->sm_count = prop.multiProcessorCount;
+    for (int p = 0; p < 2; p++) {
+        cudaEventCreateWithFlags(&e->h2d_done[p], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&e->step_done[p], cudaEventDisableTiming);
+    }
+    cudaEventCreate(&e->k_start);
+    cudaEventCreate(&e->k_end);
+    if (cfg->warps_per_cta > 0) {
+        e->warps = cfg->warps_per_cta;
+        e->ctas = cfg->max_ctas;
+        e->tuned = true;
+    } else {
+        /* launch shapes tried on the first steps: warps per CTA x grid cap
+         * in waves of resident CTAs (0 = one CTA per work chunk) */
+        const int wl[3] = { 2, 4, 8 };
+        for (int w : wl) {
+            e->tune_cands.push_back({ w, 0 });
+            e->tune_cands.push_back({ w, e->sm_count * (64 / w) });
+        }
+    }
+    *out = e;
+    return H261B_OK;
+}
+
+extern "C" int h261b_engine_destroy(h261b_engine_t *e)
+{
+    if (!e)
+        return H261B_OK;
+    cudaSetDevice(e->cfg.device);
+    cudaStreamSynchronize(e->stream);
+    for (int p = 0; p < 2; p++) {
+        e->upload[p].release();
+        e->results[p].release();
+        e->desc[p].release();
+        cudaEventDestroy(e->h2d_done[p]);
+        cudaEventDestroy(e->step_done[p]);
+    }
+    cudaEventDestroy(e->k_start);
+    cudaEventDestroy(e->k_end);
+    cudaStreamDestroy(e->stream);
+    delete e;
+    return H261B_OK;
+}
+
+static Session *get_session(h261b_engine_t *e, int32_t id)
+{
+    if (!e || id < 0 || id >= (int32_t)e->sessions.size() || !e->sessions[(size_t)id].open) {
+        set_error("invalid session id %d", id);
+        return nullptr;
+    }
+    return &e->sessions[(size_t)id];
+}
+
+extern "C" int h261b_session_open(h261b_engine_t *e, const h261b_session_config_t *c, int32_t *id)
+{
+    clear_error();
+    if (!e || !c || !id || c->width < 16 || c->height < 16 || (c->width & 15) || (c->height & 15) ||
+        (c->width / 16) * (c->height / 16) > H261B_MAX_MB_PER_SESSION || c->quant < 1 || c->quant > 31 ||
+        c->intra_period < 0 || c->denoise < 0) {
+        set_error("h261b_session_open: bad session configuration");
+        return H261B_ERR_ARG;
+    }
+    const int64_t need = h261b_session_bytes(c->width, c->height);
+    if (e->cfg.hbm_budget_bytes > 0 && e->session_bytes + need > e->cfg.hbm_budget_bytes) {
+        set_error("h261b_session_open: HBM budget %lld exceeded", (long long)e->cfg.hbm_budget_bytes);
+        return H261B_ERR_BUDGET;
+    }
+    int32_t slot = -1;
+    for (size_t i = 0; i < e->sessions.size(); i++)
+        if (!e->sessions[i].open) {
+            slot = (int32_t)i;
+            break;
+        }
+    if (slot < 0) {
+        set_error("h261b_session_open: all %d session slots in use", e->cfg.max_sessions);
+        return H261B_ERR_BUDGET;
+    }
+    cudaSetDevice(e->cfg.device);
+    Session &s = e->sessions[(size_t)slot];
+    s = Session();
+    s.w = c->width;
+    s.h = c->height;
+    s.mbw = c->width / 16;
+    s.mbh = c->height / 16;
+    s.nmb = s.mbw * s.mbh;
+    s.quant = c->quant;
+    s.intra_period = c->intra_period;
+    s.lay = PictureLayout::of(s.w, s.h);
+    s.slot_bytes = (size_t)need;
+    void *blk = nullptr;
+    int rc = e->pool.get(s.slot_bytes, &blk);
+    if (rc != H261B_OK)
+        return rc;
+    uint8_t *base = (uint8_t *)blk;
+    s.rec[0] = base;
+    s.rec[1] = base + s.lay.bytes;
+    s.dn = (h261b_denoise_dev_t *)(base + 2 * s.lay.bytes);
+    /* the first reference is black like the reference's zeroed frame
+     * (h261_main.c:155-157); denoise state starts at zero
+     * (gpu_device.cu:495-508) */
+    h261b_denoise_dev_t dn0;
+    memset(&dn0, 0, sizeof(dn0));
+    dn0.denoise = c->denoise;
+    H261B_CUDA_TRY(cudaMemsetAsync(base, 0, 2 * s.lay.bytes, e->stream));
+    H261B_CUDA_TRY(cudaMemcpyAsync(s.dn, &dn0, sizeof(dn0), cudaMemcpyHostToDevice, e->stream));
+    H261B_CUDA_TRY(cudaStreamSynchronize(e->stream));
+    s.open = true;
+    e->open_count++;
+    e->session_bytes += need;
+    *id = slot;
+    return H261B_OK;
+}
+
+extern "C" int h261b_session_close(h261b_engine_t *e, int32_t id)
+{
+    clear_error();
+    Session *s = get_session(e, id);
+    if (!s)
+        return H261B_ERR_ARG;
+    /* a step may still read the session's pictures */
+    H261B_CUDA_TRY(cudaStreamSynchronize(e->stream));
+    e->pool.put(s->slot_bytes, s->rec[0]);
+    e->session_bytes -= (int64_t)s->slot_bytes;
+    e->open_count--;
+    *s = Session();
+    return H261B_OK;
+}
+
+/* grow the arenas of parity p to hold a step of every open session; the
+ * queued part of the upload arena is kept, results of the other parity
+ * (the last step, still readable by the caller) are not touched */
+static int ensure_capacity(h261b_engine_t *e, int p)
+{
+    size_t up = 0, res = 0;
+    int32_t n = 0;
+    for (const Session &s : e->sessions)
+        if (s.open) {
+            up += align_up(s.lay.bytes, 256);
+            res += align_up((size_t)s.nmb * sizeof(h261b_mb_info_t), 256) + align_up((size_t)s.nmb * 384, 256);
+            n++;
+        }
+    const size_t desc = align_up((size_t)n * sizeof(h261b_session_dev_t), 256) +
+                        (size_t)n * H261B_MAX_MB_PER_SESSION * sizeof(uint32_t);
+    if (up > e->upload[p].cap || res > e->results[p].cap || desc > e->desc[p].cap) {
+        H261B_CUDA_TRY(cudaStreamSynchronize(e->stream));
+        int rc;
+        const size_t keep = (p == e->parity && e->upload_checked) ? e->upload_used : 0;
+        if ((rc = e->upload[p].reserve(up, keep)) || (rc = e->results[p].reserve(res)) ||
+            (rc = e->desc[p].reserve(desc)))
+            return rc;
+    }
+    return H261B_OK;
+}
+
+extern "C" int h261b_session_submit(h261b_engine_t *e, int32_t id, const uint8_t *y, const uint8_t *cb,
+                                    const uint8_t *cr, int32_t quant)
+{
+    clear_error();
+    Session *s = get_session(e, id);
+    if (!s || !y || !cb || !cr || quant > 31) {
+        if (s)
+            set_error("h261b_session_submit: bad argument");
+        return H261B_ERR_ARG;
+    }
+    if (s->queued) {
+        set_error("h261b_session_submit: session %d already has a queued picture", id);
+        return H261B_ERR_STATE;
+    }
+    int rc = ensure_capacity(e, e->parity);
+    if (rc)
+        return rc;
+    Mirror &up = e->upload[e->parity];
+    if (!e->upload_checked) {
+        /* the copy that last read this pinned arena must be complete */
+        if (e->in_flight[e->parity])
+            H261B_CUDA_TRY(cudaEventSynchronize(e->h2d_done[e->parity]));
+        e->upload_checked = true;
+        e->upload_used = 0;
+    }
+    const size_t off = e->upload_used;
+    if (off + s->lay.bytes > up.cap) {
+        set_error("h261b_session_submit: upload arena overflow");
+        return H261B_ERR_STATE;
+    }
+    const size_t ny = (size_t)s->w * s->h, nc = ny / 4;
+    memcpy(up.host + off + s->lay.off_y, y, ny);
+    memcpy(up.host + off + s->lay.off_cb, cb, nc);
+    memcpy(up.host + off + s->lay.off_cr, cr, nc);
+    e->upload_used = off + align_up(s->lay.bytes, 256);
+    s->src_off = off;
+    s->queued = true;
+    s->queued_quant = quant > 0 ? quant : 0;
+    return H261B_OK;
+}
+
+extern "C" int h261b_session_submit_device(h261b_engine_t *e, int32_t id, const uint8_t *y, const uint8_t *cb,
+                                           const uint8_t *cr, int32_t quant)
+{
+    clear_error();
+    Session *s = get_session(e, id);
+    if (!s || !y || !cb || !cr || quant > 31)
+        return H261B_ERR_ARG;
+    /* 16-byte luma rows and 8-byte chroma rows are loaded whole */
+    if (((uintptr_t)y & 15) || ((uintptr_t)cb & 7) || ((uintptr_t)cr & 7)) {
+        set_error("h261b_session_submit_device: planes must be 16 (Y) and 8 (Cb, Cr) byte aligned");
+        return H261B_ERR_ARG;
+    }
+    if (s->queued) {
+        set_error("h261b_session_submit_device: session %d already has a queued picture", id);
+        return H261B_ERR_STATE;
+    }
+    s->dev_src[0] = y;
+    s->dev_src[1] = cb;
+    s->dev_src[2] = cr;
+    s->queued = true;
+    s->queued_quant = quant > 0 ? quant : 0;
+    return H261B_OK;
+}
+
+static int next_launch_shape(h261b_engine_t *e, int *warps, int *ctas)
+{
+    if (!e->tuned && e->tune_next < e->tune_cands.size()) {
+        *warps = e->tune_cands[e->tune_next].first;
+        *ctas = e->tune_cands[e->tune_next].second;
+        return 1;
+    }
+    *warps = e->warps;
+    *ctas = e->ctas;
+    return 0;
+}
+
+extern "C" int h261b_engine_step(h261b_engine_t *e)
+{
+    clear_error();
+    if (!e)
+        return H261B_ERR_ARG;
+    cudaSetDevice(e->cfg.device);
+    const int p = e->parity;
+    std::vector<int32_t> list;
+    for (size_t i = 0; i < e->sessions.size(); i++)
+        if (e->sessions[i].open && e->sessions[i].queued)
+            list.push_back((int32_t)i);
+    if (list.empty())
+        return 0;
+    int rc = ensure_capacity(e, p);
+    if (rc)
+        return rc;
+    /* results and descriptors of this parity were last used two steps ago */
+    if (e->in_flight[p])
+        H261B_CUDA_TRY(cudaEventSynchronize(e->step_done[p]));
+
+    Mirror &dm = e->desc[p], &rm = e->results[p], &um = e->upload[p];
+    const size_t n = list.size();
+    h261b_session_dev_t *desc = (h261b_session_dev_t *)dm.host;
+    const size_t work_off = align_up(n * sizeof(h261b_session_dev_t), 256);
+    uint32_t *work = (uint32_t *)(dm.host + work_off);
+    size_t res_off = 0;
+    int32_t n_work = 0;
+    for (size_t k = 0; k < n; k++) {
+        Session &s = e->sessions[(size_t)list[k]];
+        if (s.queued_quant > 0)
+            s.quant = s.queued_quant;
+        const int intra = s.frame_index == 0 || (s.intra_period > 0 && s.frame_index % s.intra_period == 0);
+        const uint8_t *src = um.dev + s.src_off;
+        const uint8_t *ref = s.rec[s.rec_cur];
+        uint8_t *rec = s.rec[s.rec_cur ^ 1];
+        h261b_session_dev_t &d = desc[k];
+        memset(&d, 0, sizeof(d));
+        if (s.dev_src[0]) {
+            d.cur_y = s.dev_src[0];
+            d.cur_cb = s.dev_src[1];
+            d.cur_cr = s.dev_src[2];
+        } else {
+            d.cur_y = src + s.lay.off_y;
+            d.cur_cb = src + s.lay.off_cb;
+            d.cur_cr = src + s.lay.off_cr;
+        }
+        d.ref_y = ref + s.lay.off_y;
+        d.ref_cb = ref + s.lay.off_cb;
+        d.ref_cr = ref + s.lay.off_cr;
+        d.rec_y = rec + s.lay.off_y;
+        d.rec_cb = rec + s.lay.off_cb;
+        d.rec_cr = rec + s.lay.off_cr;
+        d.pitch_y = s.lay.pitch_y;
+        d.pitch_c = s.lay.pitch_c;
+        d.mbw = s.mbw;
+        d.mbh = s.mbh;
+        d.frame_type = intra ? H261B_FRAME_TYPE_INTRA : H261B_FRAME_TYPE_INTER;
+        d.quant = s.quant;
+        d.me_mode = e->cfg.me_mode;
+        d.skip_search = intra;
+        d.dn = s.dn;
+        s.info_off = res_off;
+        d.info_out = (h261b_mb_info_t *)(rm.dev + res_off);
+        res_off += align_up((size_t)s.nmb * sizeof(h261b_mb_info_t), 256);
+        s.level_off = res_off;
+        d.level_out = (int8_t *)(rm.dev + res_off);
+        res_off += align_up((size_t)s.nmb * 384, 256);
+        for (int32_t m = 0; m < s.nmb; m++)
+            work[n_work++] = ((uint32_t)k << 12) | (uint32_t)m;
+        s.res_frame = s.frame_index;
+        s.res_type = d.frame_type;
+        s.res_quant = s.quant;
+        s.res_parity = p;
+    }
+    const size_t desc_bytes = work_off + (size_t)n_work * sizeof(uint32_t);
+    H261B_CUDA_TRY(cudaMemcpyAsync(dm.dev, dm.host, desc_bytes, cudaMemcpyHostToDevice, e->stream));
+    if (e->upload_used)
+        H261B_CUDA_TRY(cudaMemcpyAsync(um.dev, um.host, e->upload_used, cudaMemcpyHostToDevice, e->stream));
+    H261B_CUDA_TRY(cudaEventRecord(e->h2d_done[p], e->stream));
+
+    int warps, ctas;
+    const int tuning = next_launch_shape(e, &warps, &ctas);
+    H261B_CUDA_TRY(cudaEventRecord(e->k_start, e->stream));
+    const int phases = H261B_PHASE_ME | H261B_PHASE_MD | H261B_PHASE_ENCDEC | (e->cfg.fmad ? 0x100 : 0);
+    int lr = h261b_launch_step((const h261b_session_dev_t *)dm.dev, (const uint32_t *)(dm.dev + work_off), n_work,
+                               phases, warps, ctas, e->stream);
+    if (lr != 0) {
+        set_error("step launch failed: %s", cudaGetErrorString((cudaError_t)lr));
+        return H261B_ERR_CUDA;
+    }
+    H261B_CUDA_TRY(cudaEventRecord(e->k_end, e->stream));
+    H261B_CUDA_TRY(cudaMemcpyAsync(rm.host, rm.dev, res_off, cudaMemcpyDeviceToHost, e->stream));
+    H261B_CUDA_TRY(cudaEventRecord(e->step_done[p], e->stream));
+    e->in_flight[p] = true;
+
+    if (tuning) {
+        /* time this candidate before moving on (tuning steps are synchronous) */
+        H261B_CUDA_TRY(cudaEventSynchronize(e->k_end));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e->k_start, e->k_end);
+        e->tune_ms.push_back(ms);
+        e->tune_next++;
+        if (e->tune_next == e->tune_cands.size()) {
+            size_t best = 0;
+            for (size_t i = 1; i < e->tune_ms.size(); i++)
+                if (e->tune_ms[i] < e->tune_ms[best])
+                    best = i;
+            e->warps = e->tune_cands[best].first;
+            e->ctas = e->tune_cands[best].second;
+            e->tuned = true;
+        }
+    }
+
+    for (int32_t id : list) {
+        Session &s = e->sessions[(size_t)id];
+        s.queued = false;
+        s.queued_quant = 0;
+        s.dev_src[0] = s.dev_src[1] = s.dev_src[2] = nullptr;
+        s.rec_cur ^= 1;
+        s.frame_index++;
+        s.has_result = false;
+    }
+    e->last_stepped = list;
+    e->last_parity = p;
+    e->parity ^= 1;
+    e->upload_checked = false;
+    e->upload_used = 0;
+    return (int)n;
+}
+
+extern "C" int h261b_engine_sync(h261b_engine_t *e)
+{
+    clear_error();
+    if (!e)
+        return H261B_ERR_ARG;
+    if (e->last_parity < 0)
+        return H261B_OK;
+    H261B_CUDA_TRY(cudaEventSynchronize(e->step_done[e->last_parity]));
+    for (int32_t id : e->last_stepped)
+        e->sessions[(size_t)id].has_result = true;
+    return H261B_OK;
+}
+
+extern "C" int h261b_session_result(h261b_engine_t *e, int32_t id, h261b_frame_result_t *out)
+{
+    clear_error();
+    Session *s = get_session(e, id);
+    if (!s || !out)
+        return H261B_ERR_ARG;
+    if (!s->has_result) {
+        set_error("h261b_session_result: no completed step for session %d (call h261b_engine_sync)", id);
+        return H261B_ERR_STATE;
+    }
+    const Mirror &rm = e->results[s->res_parity];
+    out->frame_index = s->res_frame;
+    out->frame_type = s->res_type;
+    out->quant = s->res_quant;
+    out->num_mb = s->nmb;
+    out->mbs = (const h261b_mb_result_t *)(rm.host + s->info_off);
+    out->levels = (const int8_t *)(rm.host + s->level_off);
+    return H261B_OK;
+}
+
+extern "C" int h261b_session_recon(h261b_engine_t *e, int32_t id, uint8_t *y, uint8_t *cb, uint8_t *cr)
+{
+    clear_error();
+    Session *s = get_session(e, id);
+    if (!s || !y || !cb || !cr)
+        return H261B_ERR_ARG;
+    cudaSetDevice(e->cfg.device);
+    H261B_CUDA_TRY(cudaStreamSynchronize(e->stream));
+    const uint8_t *rec = s->rec[s->rec_cur];
+    const size_t ny = (size_t)s->w * s->h, nc = ny / 4;
+    H261B_CUDA_TRY(cudaMemcpy(y, rec + s->lay.off_y, ny, cudaMemcpyDeviceToHost));
+    H261B_CUDA_TRY(cudaMemcpy(cb, rec + s->lay.off_cb, nc, cudaMemcpyDeviceToHost));
+    H261B_CUDA_TRY(cudaMemcpy(cr, rec + s->lay.off_cr, nc, cudaMemcpyDeviceToHost));
+    return H261B_OK;
+}
+
+extern "C" int h261b_result_to_abi(const h261b_frame_result_t *r, int32_t width, h261_macroblock_t *mbs)
+{
+    if (!r || !mbs || width < 16 || (width & 15))
+        return H261B_ERR_ARG;
+    const int32_t mbw = width / 16;
+    for (int32_t i = 0; i < r->num_mb; i++) {
+        const h261b_mb_result_t &m = r->mbs[i];
+        h261_macroblock_t &o = mbs[i];
+        o.i_macroblock_address = 0;
+        o.i_macroblock_type = m.type;
+        o.i_macroblock_type_flags = m.flags;
+        o.i_macroblock_quant = m.quant;
+        o.rgi_mv[0] = m.mvx;
+        o.rgi_mv[1] = m.mvy;
+        o.i_coded_block_pattern = (uint8_t)m.cbp;
+        const int8_t *lv = r->levels + (size_t)i * 384;
+        for (int b = 0; b < 6; b++)
+            for (int k = 0; k < 64; k++)
+                o.rgi_tcoeff[b][k] = lv[b * 64 + k];
+        if (m.type == H261B_MB_TYPE_INTRA)
+            for (int b = 0; b < 6; b++)
+                o.rgi_tcoeff[b][0] = (uint8_t)lv[b * 64];
+        o.i_mb_x = (i % mbw) * 16;
+        o.i_mb_y = (i / mbw) * 16;
+    }
+    return H261B_OK;
+}
+
+extern "C" int h261b_engine_last_kernel_ms(h261b_engine_t *e, float *ms)
+{
+    if (!e || !ms)
+        return H261B_ERR_ARG;
+    H261B_CUDA_TRY(cudaEventSynchronize(e->k_end));
+    H261B_CUDA_TRY(cudaEventElapsedTime(ms, e->k_start, e->k_end));
+    return H261B_OK;
+}
+
+extern "C" int h261b_engine_stats(h261b_engine_t *e, int32_t *open_sessions, int32_t *queued, int64_t *bytes)
+{
+    if (!e)
+        return H261B_ERR_ARG;
+    int32_t q = 0;
+    for (const Session &s : e->sessions)
+        q += s.open && s.queued;
+    if (open_sessions)
+        *open_sessions = e->open_count;
+    if (queued)
+        *queued = q;
+    if (bytes)
+        *bytes = e->pool.held();
+    return H261B_OK;
+}

@@ -1,0 +1,84 @@
+/*
+ * h261b_device.h -- descriptors shared by the host engine and the kernels.
+ *
+ * Device memory model (all in HBM, nothing re-uploaded per frame):
+ *   picture   three planes; luma pitch = W, chroma pitch = W/2 rounded up
+ *             to 16 bytes, every plane 256-byte aligned;
+ *   session   one encode stream: a source picture per in-flight frame, two
+ *             reconstruction pictures that alternate as reference / output,
+ *             and its denoise state;
+ *   step      one picture of every participating session; a flat list of
+ *             (session, MB) work items covers the step.
+ */
+#ifndef H261B_DEVICE_H
+#define H261B_DEVICE_H
+
+#include <stdint.h>
+#include "../../include/h261b_abi.h"
+
+#define H261B_MAX_MB_PER_SESSION 4096
+
+/* per-session denoise state: the reference's h261_dct_denoise_t
+ * (src/h261_types.h:122-132) split into this frame's offsets and the
+ * accumulators of the frame being coded, plus the frame-end ticket */
+typedef struct {
+    int32_t denoise;
+    uint32_t ticket;          /* MBs of the current frame finished          */
+    int32_t count[2];         /* blocks coded this frame: [0] intra [1] inter */
+    int32_t noise[2][64];     /* sum of |coefficient| before shrinking       */
+    int32_t offset[2][64];    /* shrink offsets used by the current frame    */
+} h261b_denoise_dev_t;
+
+/* compact per-MB result of the batched path (16 bytes) */
+typedef struct {
+    int16_t type;             /* H261B_MB_TYPE_INTRA / _INTER                */
+    int16_t flags;            /* MC | FILTER | COEFF                          */
+    int8_t quant;
+    int8_t cbp;
+    int8_t mvx, mvy;
+    int32_t cost;             /* mode-decision cost (rate control input)     */
+    int32_t reserved;
+} h261b_mb_info_t;
+
+typedef struct {
+    /* pictures */
+    const uint8_t *cur_y, *cur_cb, *cur_cr;
+    const uint8_t *ref_y, *ref_cb, *ref_cr;
+    uint8_t *rec_y, *rec_cb, *rec_cr;
+    int32_t pitch_y, pitch_c;
+    int32_t mbw, mbh;
+    /* picture parameters */
+    int32_t frame_type;       /* H261B_FRAME_TYPE_INTRA / _INTER             */
+    int32_t quant;            /* picture QUANT, 1..31                         */
+    int32_t me_mode;          /* 0 reference two-stage search, 1 full search */
+    int32_t skip_search;      /* 1: intra picture, leave ME results unset    */
+    h261b_denoise_dev_t *dn;
+    /* inputs of the encode-only phase (ABI path): host mode decision */
+    const h261_mb_mode_decision_t *md_in;
+    /* outputs, any may be NULL */
+    me_gpu_mb_t *me_out;          /* ME results per MB                      */
+    me_gpu_mv_t *stage1_out;      /* stage-1 vector per MB                  */
+    h261_mb_mode_decision_t *md_out;
+    h261_macroblock_t *abi_out;   /* reference layout, int32 levels         */
+    h261b_mb_info_t *info_out;    /* compact layout                         */
+    int8_t *level_out;            /* [nmb][6][64]; intra DC stored as uint8  */
+} h261b_session_dev_t;
+
+/* phases a launch runs for each MB */
+#define H261B_PHASE_ME      1     /* search + cost evaluation               */
+#define H261B_PHASE_MD      2     /* device mode decision                   */
+#define H261B_PHASE_ENCDEC  4     /* MC, FDCT, denoise, quant, IDCT, recon  */
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+/* host-side launchers (kernels.cu); return a cudaError_t value */
+int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const uint32_t *work_dev,
+                      int32_t n_work, int32_t phases, int32_t warps_per_cta, int32_t max_ctas,
+                      void *stream);
+int h261b_set_quant_table(void);
+#ifdef __cplusplus
+}
+#endif
+
+#endif

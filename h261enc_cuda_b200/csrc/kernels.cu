@@ -1,0 +1,900 @@
+/*
+ * kernels.cu -- the sm_100a encode core: one warp per macroblock.
+ *
+ * A launch covers a flat list of (session, MB) work items, one frame-step
+ * of any number of sessions of mixed size.  Each warp takes work items in a
+ * grid-stride loop and runs, for its MB, the phases the launch asks for:
+ *
+ *   ME      stage the 46x48 luma search window and the source MB in shared
+ *           memory (16-byte loads), then
+ *             - reference mode: SAD over the 11x11 coarse grid of
+ *               megpu_kernels.cuh:27-166, then the 7x7 refinement of
+ *               :307-446 around its winner;
+ *             - full mode: every vector of [-15,15]^2;
+ *           four packed pixels per step (__vabsdiffu4 + __dp4a on funnel-
+ *           shifted words).  The reference picks a winner with a 2-D tree of strict
+ *           '<' comparisons in the order self, right, below, diagonal
+ *           (:95-154); that tree returns the minimum cost and, among equal
+ *           costs, the cell with the smallest Z-order index (x bits on even
+ *           positions).  Each lane therefore folds (cost << 10 | zorder) into
+ *           one 32-bit key and a single redux.sync min picks the same winner.
+ *           Then the three 16x16 SATD costs of :617-987 (inter, inter with
+ *           the 3x3 interior filter, intra).
+ *   MD      the decision of h261_moded.c:53-95.
+ *   ENCDEC  per 8x8 block, one lane per row then per column: prediction
+ *           with the H.261 loop filter, the reference's float/double AAN
+ *           FDCT (mbgpu_kernels.cuh:337-442) with every rounding step
+ *           spelled out by intrinsics, denoise against the session's
+ *           offsets (:506-636), quantisation (:644-724), dequantisation
+ *           (:731-815), the AAN IDCT (:827-931) and reconstruction
+ *           (:988-1277) into the session's output picture.  The last warp to
+ *           finish a session's frame turns the frame's denoise statistics
+ *           into the next frame's offsets (:478-503).
+ *
+ * No warp waits on another: the frame-end update is a ticket taken after a
+ * warp's statistics are published, so a launch never spins.
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "h261b_device.h"
+
+namespace {
+
+constexpr int WIN_ROWS = 46;        /* rows mb_y-15 .. mb_y+30              */
+constexpr int WIN_PITCH_W = 13;     /* 48 columns in 13 words (odd pitch)    */
+constexpr uint32_t FULL = 0xffffffffu;
+
+struct __align__(16) WarpSmem {
+    uint32_t win[WIN_ROWS * WIN_PITCH_W]; /* reference luma window          */
+    uint32_t pad0[2];
+    uint32_t cur[64];                     /* source luma MB, 16 B per row   */
+    uint32_t curc[2][16];                 /* source Cb, Cr 8x8               */
+    float t[4][64];                       /* transpose buffer               */
+};
+
+__constant__ int8_t c_stage1[11] = { -14, -11, -8, -5, -2, 0, 2, 5, 8, 11, 14 };
+/* float tables initialised from double literals like the reference's */
+__constant__ float c_fwd_post[8] = { 1.0, 0.720960, 0.765367, 0.850430, 1.0, 1.272759, 1.847759, 3.624510 };
+__constant__ float c_inv_pre[8] = { 1.0, 1.387040, 1.306563, 1.175876, 1.0, 0.785695, 0.541196, 0.275899 };
+__constant__ float c_inv_quant[32];
+
+/* ------------------------------------------------------------ helpers */
+
+__device__ __forceinline__ uint32_t spread8(uint32_t v)
+{
+    v &= 0xFFu;
+    v = (v | (v << 4)) & 0x0F0Fu;
+    v = (v | (v << 2)) & 0x3333u;
+    v = (v | (v << 1)) & 0x5555u;
+    return v;
+}
+
+__device__ __forceinline__ uint32_t compact8(uint32_t v)
+{
+    v &= 0x5555u;
+    v = (v | (v >> 1)) & 0x3333u;
+    v = (v | (v >> 2)) & 0x0F0Fu;
+    v = (v | (v >> 4)) & 0x00FFu;
+    return v;
+}
+
+__device__ __forceinline__ uint32_t zorder(uint32_t x, uint32_t y) { return spread8(x) | (spread8(y) << 1); }
+
+__device__ __forceinline__ uint8_t win_byte(const WarpSmem &s, int row, int col)
+{
+    return reinterpret_cast<const uint8_t *>(s.win)[row * (WIN_PITCH_W * 4) + col];
+}
+
+__device__ __forceinline__ uint8_t cur_byte(const WarpSmem &s, int row, int col)
+{
+    return reinterpret_cast<const uint8_t *>(s.cur)[row * 16 + col];
+}
+
+/* sum of |a_i - b_i| over the four bytes, added to acc: per-byte absolute
+ * difference, then a dot product with 1,1,1,1 (measured on B200 faster
+ * than __vsadu4) */
+__device__ __forceinline__ uint32_t sad4(uint32_t a, uint32_t b, uint32_t acc)
+{
+    return __dp4a(__vabsdiffu4(a, b), 0x01010101u, acc);
+}
+
+/* SAD of the source MB against the window block at vector (vx, vy) */
+__device__ __forceinline__ uint32_t sad16x16(const WarpSmem &s, int vx, int vy)
+{
+    const int bo = 16 + vx;
+    const uint32_t *p = s.win + (15 + vy) * WIN_PITCH_W + (bo >> 2);
+    const uint32_t sh = (uint32_t)(bo & 3) * 8u;
+    uint32_t acc = 0;
+#pragma unroll 4
+    for (int r = 0; r < 16; r++) {
+        const uint32_t a0 = p[0], a1 = p[1], a2 = p[2], a3 = p[3], a4 = p[4];
+        const uint4 c = *reinterpret_cast<const uint4 *>(s.cur + 4 * r);
+        acc = sad4(c.x, __funnelshift_r(a0, a1, sh), acc);
+        acc = sad4(c.y, __funnelshift_r(a1, a2, sh), acc);
+        acc = sad4(c.z, __funnelshift_r(a2, a3, sh), acc);
+        acc = sad4(c.w, __funnelshift_r(a3, a4, sh), acc);
+        p += WIN_PITCH_W;
+    }
+    return acc;
+}
+
+/* 4x4 Hadamard SATD, megpu_kernels.cuh:467-500 */
+__device__ __forceinline__ int32_t satd4x4(const int32_t d[16])
+{
+    int32_t t[16];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int32_t a1 = d[4 * i] + d[4 * i + 1], a2 = d[4 * i] - d[4 * i + 1];
+        const int32_t a3 = d[4 * i + 2] + d[4 * i + 3], a4 = d[4 * i + 2] - d[4 * i + 3];
+        t[4 * i + 0] = a1 + a3;
+        t[4 * i + 1] = a2 + a4;
+        t[4 * i + 2] = a1 - a3;
+        t[4 * i + 3] = a2 - a4;
+    }
+    int32_t satd = 0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int32_t a1 = t[i] + t[4 + i], a2 = t[i] - t[4 + i];
+        const int32_t a3 = t[8 + i] + t[12 + i], a4 = t[8 + i] - t[12 + i];
+        satd += abs(a1 + a3) + abs(a2 + a4) + abs(a1 - a3) + abs(a2 - a4);
+    }
+    return satd;
+}
+
+/* ---------------------------------------------- exact float/double math */
+
+/* `float *= double`: double product rounded to float */
+__device__ __forceinline__ float dmulf(float x, double k)
+{
+    return __double2float_rn(__dmul_rn((double)x, k));
+}
+
+/* `float = float * double + float`: fused (one rounding) or not */
+template <int FMAD>
+__device__ __forceinline__ float dmadf(float a, double k, float c)
+{
+    if (FMAD)
+        return __double2float_rn(__fma_rn((double)a, k, (double)c));
+    return __double2float_rn(__dadd_rn(__dmul_rn((double)a, k), (double)c));
+}
+
+/* the AAN forward butterfly shared by both passes (mbgpu_kernels.cuh:359-388) */
+template <int FMAD>
+__device__ __forceinline__ void fdct_butterfly(float tmp0, float tmp1, float tmp2, float tmp3, float tmp4,
+                                               float tmp5, float tmp6, float tmp7, float o[8])
+{
+    const float tmp10 = tmp0 + tmp3, tmp13 = tmp0 - tmp3, tmp11 = tmp1 + tmp2, tmp12 = tmp1 - tmp2;
+    o[0] = tmp10 + tmp11;
+    o[4] = tmp10 - tmp11;
+    const float z1 = dmulf(tmp12 + tmp13, 0.707107);
+    o[2] = tmp13 + z1;
+    o[6] = tmp13 - z1;
+    tmp4 = tmp4 + tmp5;
+    tmp5 = tmp5 + tmp6;
+    tmp6 = tmp6 + tmp7;
+    const float z5 = dmulf(tmp4 - tmp6, 0.382683);
+    const float z2 = dmadf<FMAD>(tmp4, 0.541196, z5);
+    const float z4 = dmadf<FMAD>(tmp6, 1.306563, z5);
+    const float z3 = dmulf(tmp5, 0.707107);
+    const float z11 = tmp7 + z3, z13 = tmp7 - z3;
+    o[5] = z13 + z2;
+    o[3] = z13 - z2;
+    o[1] = z11 + z4;
+    o[7] = z11 - z4;
+}
+
+/* floorf( cs * post * v + 0.49999 ): float product, double sum, float floor */
+__device__ __forceinline__ int32_t fdct_round(float cs, float post, float v)
+{
+    const float prod = __fmul_rn(__fmul_rn(cs, post), v);
+    return __float2int_rz(floorf(__double2float_rn(__dadd_rn((double)prod, 0.49999))));
+}
+
+/* the AAN inverse butterfly after its first level of adds (mbgpu_kernels.cuh
+ * :851-887 for columns, :892-919 for rows); the caller forms the first level
+ * (tmp12 = p2 - p6, tmp13 = p2 + p6, tmp10 = p0 + p4, tmp11 = p0 - p4,
+ * z11 = p1 + p7, z12 = p1 - p7, z13 = p5 + p3, z10 = p5 - p3) */
+template <int FMAD>
+__device__ __forceinline__ void idct_rest(float tmp12, float tmp13, float tmp10, float tmp11, float z11,
+                                          float z12, float z13, float z10, float o[8])
+{
+    tmp12 = dmulf(tmp12, 1.414214);
+    tmp12 = tmp12 - tmp13;
+    const float tmp0 = tmp10 + tmp13, tmp1 = tmp11 + tmp12, tmp2 = tmp11 - tmp12, tmp3 = tmp10 - tmp13;
+    tmp13 = z11 + z13;
+    tmp11 = dmulf(z11 - z13, 1.414214);
+    const float z5 = dmulf(z12 + z10, 1.84776);
+    tmp10 = dmadf<FMAD>(z12, 1.082392, -z5);
+    tmp12 = dmadf<FMAD>(z10, -2.613126, z5);
+    tmp12 = tmp12 - tmp13;
+    tmp11 = tmp11 - tmp12;
+    tmp10 = tmp10 + tmp11;
+    o[0] = tmp0 + tmp13;
+    o[1] = tmp1 + tmp12;
+    o[2] = tmp2 + tmp11;
+    o[3] = tmp3 - tmp10;
+    o[4] = tmp3 + tmp10;
+    o[5] = tmp2 - tmp11;
+    o[6] = tmp1 - tmp12;
+    o[7] = tmp0 - tmp13;
+}
+
+/* first level of the column pass on prescaled products t = P * cs: the
+ * reference built with nvcc defaults fuses the left-hand product of each
+ * add into one FFMA (its product rounds once, with the sum) */
+template <int FMAD>
+__device__ __forceinline__ float first_add(float Pa, float csa, float ta, float tb)
+{
+    return FMAD ? __fmaf_rn(Pa, csa, tb) : __fadd_rn(ta, tb);
+}
+template <int FMAD>
+__device__ __forceinline__ float first_sub(float Pa, float csa, float ta, float tb)
+{
+    return FMAD ? __fmaf_rn(Pa, csa, -tb) : __fsub_rn(ta, tb);
+}
+
+/* CLAMP_255( (Int32) floor( v + 0.49999 ) ) with v widened to double */
+__device__ __forceinline__ int32_t idct_round(float v)
+{
+    const int32_t r = (int32_t)floor(__dadd_rn((double)v, 0.49999));
+    return min(255, max(-256, r));
+}
+
+/* ---------------------------------------------------------- per MB */
+
+struct MbDecision {
+    int32_t type, flags, mvx, mvy, cost;
+};
+
+__device__ __forceinline__ void load_sources(WarpSmem &s, const h261b_session_dev_t &S, int mbx, int mby,
+                                             int lane, bool need_window)
+{
+    const int W = S.mbw * 16, H = S.mbh * 16;
+    const int x0 = mbx * 16, y0 = mby * 16;
+    if (need_window) {
+        /* 46 rows x 3 chunks of 16 pixels; chunks outside the frame are
+         * zero (no search vector ever reaches them) */
+        for (int t = lane; t < WIN_ROWS * 3; t += 32) {
+            const int r = t / 3, c = t - r * 3;
+            const int y = y0 - 15 + r, x = x0 - 16 + 16 * c;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (y >= 0 && y < H && x >= 0 && x < W)
+                v = *reinterpret_cast<const uint4 *>(S.ref_y + (size_t)y * S.pitch_y + x);
+            uint32_t *d = s.win + r * WIN_PITCH_W + 4 * c;
+            d[0] = v.x;
+            d[1] = v.y;
+            d[2] = v.z;
+            d[3] = v.w;
+        }
+    }
+    if (lane < 16) {
+        const uint4 v = *reinterpret_cast<const uint4 *>(S.cur_y + (size_t)(y0 + lane) * S.pitch_y + x0);
+        *reinterpret_cast<uint4 *>(s.cur + 4 * lane) = v;
+    } else {
+        const int k = lane - 16, pl = k >> 3, r = k & 7;
+        const uint8_t *src = pl ? S.cur_cr : S.cur_cb;
+        const uint2 v = *reinterpret_cast<const uint2 *>(src + (size_t)(mby * 8 + r) * S.pitch_c + mbx * 8);
+        s.curc[pl][2 * r] = v.x;
+        s.curc[pl][2 * r + 1] = v.y;
+    }
+    __syncwarp();
+}
+
+/* motion search + SATD costs; results are warp-uniform */
+__device__ __forceinline__ void motion_estimate(const WarpSmem &s, const h261b_session_dev_t &S, int mbx,
+                                                int mby, int lane, me_gpu_mb_t &res, int8_t &s1x,
+                                                int8_t &s1y)
+{
+    const int bx = mbx * 16, by = mby * 16;
+    /* per-MB limits, gpu_device.cu:226-265 */
+    const int lminx = max(-15, -bx), lmaxx = min(15, (S.mbw - 1) * 16 - bx);
+    const int lminy = max(-15, -by), lmaxy = min(15, (S.mbh - 1) * 16 - by);
+    int vx, vy;
+    if (S.me_mode == 1) {
+        uint32_t best = FULL;
+        for (int c = lane; c < 31 * 31; c += 32) {
+            const int tx = c % 31, ty = c / 31, x = tx - 15, y = ty - 15;
+            const bool ok = x >= lminx && x <= lmaxx && y >= lminy && y <= lmaxy;
+            /* every lane computes a SAD; a vector outside the limits is replaced by
+             * (0, 0) so no address leaves the window, and its cost discarded */
+            const uint32_t sad = sad16x16(s, ok ? x : 0, ok ? y : 0);
+            const uint32_t cost = ok ? sad : 65535u;
+            best = min(best, (cost << 10) | zorder(tx, ty));
+        }
+        best = __reduce_min_sync(FULL, best) & 1023u; /* Z-order index only */
+        vx = (int)compact8(best) - 15;
+        vy = (int)compact8(best >> 1) - 15;
+        s1x = s1y = 0;
+    } else {
+        uint32_t best = FULL;
+        for (int c = lane; c < 121; c += 32) {
+            const int ty = c / 11, tx = c - ty * 11;
+            const int x = c_stage1[tx], y = c_stage1[ty];
+            const bool ok = x >= lminx && x <= lmaxx && y >= lminy && y <= lmaxy;
+            /* every lane computes a SAD; a vector outside the limits is replaced by
+             * (0, 0) so no address leaves the window, and its cost discarded */
+            const uint32_t sad = sad16x16(s, ok ? x : 0, ok ? y : 0);
+            const uint32_t cost = ok ? sad : 65535u;
+            best = min(best, (cost << 10) | zorder(tx, ty));
+        }
+        best = __reduce_min_sync(FULL, best) & 1023u; /* Z-order index only */
+        const int v1x = c_stage1[compact8(best)], v1y = c_stage1[compact8(best >> 1)];
+        s1x = (int8_t)v1x;
+        s1y = (int8_t)v1y;
+        best = FULL;
+        for (int c = lane; c < 49; c += 32) {
+            const int ty = c / 7, tx = c - ty * 7;
+            const int x = v1x + tx - 3, y = v1y + ty - 3;
+            const bool ok = x >= lminx && x <= lmaxx && y >= lminy && y <= lmaxy;
+            /* every lane computes a SAD; a vector outside the limits is replaced by
+             * (0, 0) so no address leaves the window, and its cost discarded */
+            const uint32_t sad = sad16x16(s, ok ? x : 0, ok ? y : 0);
+            const uint32_t cost = ok ? sad : 65535u;
+            best = min(best, (cost << 10) | zorder(tx, ty));
+        }
+        best = __reduce_min_sync(FULL, best) & 1023u; /* Z-order index only */
+        vx = v1x + (int)compact8(best) - 3;
+        vy = v1y + (int)compact8(best >> 1) - 3;
+    }
+
+    /* costs at the final vector: lanes 0-15 inter, 16-31 filtered inter,
+     * one 4x4 sub-block each; then intra on lanes 0-15 */
+    const int sb = lane & 15, sx = sb & 3, sy = sb >> 2;
+    const bool filt = lane >= 16;
+    int32_t d[16], di[16];
+#pragma unroll
+    for (int iy = 0; iy < 4; iy++)
+#pragma unroll
+        for (int ix = 0; ix < 4; ix++) {
+            const int cx = sx * 4 + ix, cy = sy * 4 + iy;
+            const int c = cur_byte(s, cy, cx);
+            const int wr = 15 + vy + cy, wc = 16 + vx + cx;
+            const int lx = (sx & 1) * 4 + ix, ly = (sy & 1) * 4 + iy;
+            int p;
+            if (filt && lx >= 1 && lx <= 6 && ly >= 1 && ly <= 6) {
+                p = (win_byte(s, wr - 1, wc - 1) + 2 * win_byte(s, wr - 1, wc) + win_byte(s, wr - 1, wc + 1) +
+                     2 * win_byte(s, wr, wc - 1) + 4 * win_byte(s, wr, wc) + 2 * win_byte(s, wr, wc + 1) +
+                     win_byte(s, wr + 1, wc - 1) + 2 * win_byte(s, wr + 1, wc) + win_byte(s, wr + 1, wc + 1) + 8) >> 4;
+            } else {
+                p = win_byte(s, wr, wc);
+            }
+            d[iy * 4 + ix] = c - p;
+            di[iy * 4 + ix] = c;
+        }
+    const int32_t satd = satd4x4(d), satd_i = satd4x4(di);
+    res.i_16x16_cost = (int32_t)__reduce_add_sync(FULL, filt ? 0u : (uint32_t)satd);
+    res.i_16x16_filter_cost = (int32_t)__reduce_add_sync(FULL, filt ? (uint32_t)satd : 0u);
+    res.i_intra_cost = (int32_t)__reduce_add_sync(FULL, filt ? 0u : (uint32_t)satd_i);
+    res.i_zero_cost = 0;
+    res.s_16x16_mv.i8_mx = (int8_t)vx;
+    res.s_16x16_mv.i8_my = (int8_t)vy;
+}
+
+/* h261_moded.c:53-95 */
+__device__ __forceinline__ MbDecision mode_decide(const me_gpu_mb_t &g, int frame_type)
+{
+    MbDecision m;
+    if (frame_type == H261B_FRAME_TYPE_INTRA ||
+        (g.i_intra_cost <= g.i_16x16_cost && g.i_intra_cost <= g.i_16x16_filter_cost)) {
+        m.type = H261B_MB_TYPE_INTRA;
+        m.cost = g.i_intra_cost;
+        m.flags = 0;
+        m.mvx = m.mvy = 0;
+    } else {
+        m.type = H261B_MB_TYPE_INTER;
+        if (g.i_16x16_filter_cost < g.i_16x16_cost) {
+            m.flags = H261B_MB_MC | H261B_MB_FILTER;
+            m.cost = g.i_16x16_filter_cost;
+        } else {
+            m.flags = 0;
+            m.cost = g.i_16x16_cost;
+        }
+        m.mvx = g.s_16x16_mv.i8_mx;
+        m.mvy = g.s_16x16_mv.i8_my;
+        if (m.mvx != 0 || m.mvy != 0)
+            m.flags |= H261B_MB_MC;
+    }
+    return m;
+}
+
+/* reference pixel (row, col) of the 8x8 prediction block of block b */
+struct BlockRef {
+    const WarpSmem *s;
+    const uint8_t *g; /* chroma: top-left of the block in the ref plane */
+    int pitch;
+    int wr, wc;       /* luma: top-left of the block in the window      */
+    bool luma;
+    __device__ __forceinline__ int at(int r, int c) const
+    {
+        return luma ? win_byte(*s, wr + r, wc + c) : g[r * pitch + c];
+    }
+    /* horizontal [1 2 1] with x4 edge columns, mbgpu_kernels.cuh:88-103 */
+    __device__ __forceinline__ int h(int r, int c) const
+    {
+        if (c == 0)
+            return at(r, 0) * 4;
+        if (c == 7)
+            return at(r, 7) * 4;
+        return at(r, c - 1) + at(r, c) * 2 + at(r, c + 1);
+    }
+};
+
+/* one pass over up to four blocks of the MB: lane = slot * 8 + row */
+template <int FMAD>
+__device__ __forceinline__ void encdec_pass(WarpSmem &s, const h261b_session_dev_t &S, int mb, int mbx,
+                                            int mby, const MbDecision &m, int quant, bool luma_pass, int lane,
+                                            int32_t stat[8], uint32_t &cbp)
+{
+    const bool active = luma_pass || lane < 16;
+    const int slot = lane >> 3, r = lane & 7;
+    const int b = luma_pass ? slot : 4 + (slot & 1);
+    const bool intra = m.type == H261B_MB_TYPE_INTRA;
+    const bool filter = (m.flags & H261B_MB_FILTER) != 0;
+    const int t = intra ? 0 : 1;
+
+    /* ---- prediction and residual of row r (mbgpu_kernels.cuh:59-166) */
+    BlockRef ref;
+    ref.s = &s;
+    int bx8 = 0, by8 = 0;
+    if (luma_pass) {
+        bx8 = (b & 1) * 8;
+        by8 = (b >> 1) * 8;
+        ref.luma = true;
+        ref.wr = 15 + m.mvy + by8;
+        ref.wc = 16 + m.mvx + bx8;
+        ref.g = nullptr;
+        ref.pitch = 0;
+    } else {
+        const int cmx = m.mvx / 2, cmy = m.mvy / 2; /* truncation toward zero */
+        const uint8_t *pl = (b == 4) ? S.ref_cb : S.ref_cr;
+        ref.luma = false;
+        ref.wr = ref.wc = 0;
+        ref.pitch = S.pitch_c;
+        ref.g = pl + (size_t)(mby * 8 + cmy) * S.pitch_c + (mbx * 8 + cmx);
+    }
+    int32_t pred[8], res[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+        pred[i] = 0;
+    if (active) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int c = luma_pass ? cur_byte(s, by8 + r, bx8 + i)
+                                    : reinterpret_cast<const uint8_t *>(s.curc[b - 4])[r * 8 + i];
+            if (intra) {
+                res[i] = c;
+                continue;
+            }
+            int p;
+            if (filter) {
+                if (r == 0 || r == 7)
+                    p = (ref.h(r, i) + 2) >> 2;
+                else
+                    p = (ref.h(r - 1, i) + ref.h(r, i) * 2 + ref.h(r + 1, i) + 8) >> 4;
+            } else {
+                p = ref.at(r, i);
+            }
+            pred[i] = p;
+            res[i] = c - p;
+        }
+        /* ---- FDCT pass 1 on row r */
+        float o[8];
+        fdct_butterfly<FMAD>((float)(res[0] + res[7]), (float)(res[1] + res[6]), (float)(res[2] + res[5]),
+                             (float)(res[3] + res[4]), (float)(res[3] - res[4]), (float)(res[2] - res[5]),
+                             (float)(res[1] - res[6]), (float)(res[0] - res[7]), o);
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            s.t[slot][r * 8 + k] = o[k];
+    }
+    __syncwarp();
+
+    /* ---- FDCT pass 2 on column c = r: coefficients (v, c), v = 0..7 */
+    const int c = r;
+    int32_t lev[8];
+    int32_t acc = 0;
+    int32_t nz[8];
+#pragma unroll
+    for (int v = 0; v < 8; v++) {
+        lev[v] = 0;
+        nz[v] = 0;
+    }
+    if (active) {
+        const float *p = s.t[slot] + c;
+        float o[8];
+        fdct_butterfly<FMAD>(p[0] + p[56], p[8] + p[48], p[16] + p[40], p[24] + p[32], p[24] - p[32],
+                             p[16] - p[40], p[8] - p[48], p[0] - p[56], o);
+        const float cs = dmulf(c_fwd_post[c], 0.125);
+        const float inv = c_inv_quant[quant];
+#pragma unroll
+        for (int v = 0; v < 8; v++) {
+            int32_t lv = fdct_round(cs, c_fwd_post[v], o[v]);
+            /* denoise (mbgpu_kernels.cuh:586-604): offsets as UInt16 */
+            const int32_t sign = lv >> 31;
+            lv = (lv ^ sign) - sign;
+            nz[v] = lv;
+            const int32_t off = (int32_t)(uint16_t)S.dn->offset[t][v * 8 + c];
+            lv = max(lv - off, 0);
+            lv = (lv ^ sign) - sign;
+            /* quant (mbgpu_kernels.cuh:689-716) */
+            if (intra && v == 0 && c == 0) {
+                int32_t dc = lv / 8;
+                dc = max(dc, 1);
+                dc = min(dc, 254);
+                if (dc == 128)
+                    dc = 255;
+                lev[0] = dc;
+                acc += 100;
+            } else {
+                const int32_t l = min(127, max(-127, __float2int_rz(__fmul_rn(__int2float_rn(lv), inv))));
+                lev[v] = l;
+                const int32_t al = abs(l);
+                acc += al > 1 ? 100 : al;
+            }
+        }
+    }
+    /* block sums over the 8 lanes of a block */
+    acc += __shfl_xor_sync(FULL, acc, 1);
+    acc += __shfl_xor_sync(FULL, acc, 2);
+    acc += __shfl_xor_sync(FULL, acc, 4);
+    const bool coded = active && acc > 2;
+    cbp |= __reduce_or_sync(FULL, coded ? (uint32_t)H261B_CBP_BIT(b) : 0u);
+
+    /* denoise statistics: sum the same coefficient position over blocks */
+#pragma unroll
+    for (int v = 0; v < 8; v++) {
+        int32_t x = nz[v];
+        x += __shfl_xor_sync(FULL, x, 8);
+        x += __shfl_xor_sync(FULL, x, 16);
+        stat[v] += x;
+    }
+
+    /* ---- levels out */
+    if (active) {
+        if (S.abi_out) {
+            int32_t *tc = S.abi_out[mb].rgi_tcoeff[b];
+#pragma unroll
+            for (int v = 0; v < 8; v++)
+                tc[v * 8 + c] = lev[v];
+        }
+        if (S.level_out) {
+            int8_t *lo = S.level_out + (size_t)mb * 384 + b * 64;
+#pragma unroll
+            for (int v = 0; v < 8; v++)
+                lo[v * 8 + c] = (int8_t)lev[v];
+        }
+    }
+
+    /* ---- dequant (mbgpu_kernels.cuh:763-814) and IDCT pass 1 on column c */
+    __syncwarp(); /* pass-2 reads of the transpose buffer are done */
+    if (active) {
+        const int32_t qa = coded ? ((quant - 1) | 1) : 0, qm = coded ? quant * 2 : 0;
+        float col[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            int32_t dq;
+            if (intra && k == 0 && c == 0) {
+                dq = lev[0] == 255 ? 1024 : lev[0] * 8;
+            } else {
+                int32_t l = lev[k] * qm;
+                if (l > 0)
+                    l += qa;
+                else if (l < 0)
+                    l -= qa;
+                dq = min(2047, max(-2048, l));
+            }
+            col[k] = (float)dq;
+        }
+        if (coded) {
+            /* prescale: t = (coef * pre[col]) * (pre[row] * 0.125) */
+            float P[8], cs[8], t[8], o[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                cs[k] = dmulf(c_inv_pre[k], 0.125);
+                P[k] = __fmul_rn(col[k], c_inv_pre[c]);
+                t[k] = __fmul_rn(P[k], cs[k]);
+            }
+            idct_rest<FMAD>(first_sub<FMAD>(P[2], cs[2], t[2], t[6]), first_add<FMAD>(P[2], cs[2], t[2], t[6]),
+                            first_add<FMAD>(P[0], cs[0], t[0], t[4]), first_sub<FMAD>(P[0], cs[0], t[0], t[4]),
+                            first_add<FMAD>(P[1], cs[1], t[1], t[7]), first_sub<FMAD>(P[1], cs[1], t[1], t[7]),
+                            first_add<FMAD>(P[5], cs[5], t[5], t[3]), first_sub<FMAD>(P[5], cs[5], t[5], t[3]), o);
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                s.t[slot][k * 8 + c] = o[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                s.t[slot][k * 8 + c] = col[k];
+        }
+    }
+    __syncwarp();
+
+    /* ---- IDCT pass 2 on row r and reconstruction (mbgpu_kernels.cuh:988-1096) */
+    if (active) {
+        const float *p = s.t[slot] + r * 8;
+        int32_t out[8];
+        if (coded) {
+            float o[8];
+            idct_rest<FMAD>(p[2] - p[6], p[2] + p[6], p[0] + p[4], p[0] - p[4], p[1] + p[7], p[1] - p[7],
+                            p[5] + p[3], p[5] - p[3], o);
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+                out[i] = idct_round(o[i]);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+                out[i] = (int32_t)p[i];
+        }
+        uint32_t lo = 0, hi = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int32_t v = min(255, max(0, intra ? out[i] : out[i] + pred[i]));
+            if (i < 4)
+                lo |= (uint32_t)v << (8 * i);
+            else
+                hi |= (uint32_t)v << (8 * (i - 4));
+        }
+        uint8_t *dst;
+        if (luma_pass)
+            dst = S.rec_y + (size_t)(mby * 16 + by8 + r) * S.pitch_y + mbx * 16 + bx8;
+        else
+            dst = ((b == 4) ? S.rec_cb : S.rec_cr) + (size_t)(mby * 8 + r) * S.pitch_c + mbx * 8;
+        *reinterpret_cast<uint2 *>(dst) = make_uint2(lo, hi);
+    }
+    __syncwarp();
+}
+
+/* frame-end denoise update by the session's last warp (mbgpu_kernels.cuh:478-503) */
+__device__ __forceinline__ void denoise_frame_end(h261b_denoise_dev_t *dn, int lane)
+{
+    int32_t cnt0 = 0, cnt1 = 0;
+    if (lane == 0) {
+        cnt0 = atomicExch(&dn->count[0], 0);
+        cnt1 = atomicExch(&dn->count[1], 0);
+    }
+    cnt0 = __shfl_sync(FULL, cnt0, 0);
+    cnt1 = __shfl_sync(FULL, cnt1, 0);
+    for (int p = lane; p < 64; p += 32) {
+        const int32_t n1 = atomicExch(&dn->noise[1][p], 0);
+        const int32_t n0 = atomicExch(&dn->noise[0][p], 0);
+        dn->offset[1][p] = (cnt1 * dn->denoise + n1 / 2) / (n1 + 1);
+        dn->offset[0][p] = (cnt0 * dn->denoise + n0 / 2) / (n0 + 1);
+    }
+    __threadfence();
+    if (lane == 0)
+        atomicExch(&dn->ticket, 0u);
+}
+
+template <int FMAD>
+__global__ void __launch_bounds__(256) step_kernel(const h261b_session_dev_t *__restrict__ sessions,
+                                                   const uint32_t *__restrict__ work, int32_t n_work,
+                                                   int32_t phases)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    WarpSmem &s = reinterpret_cast<WarpSmem *>(smem_raw)[warp];
+    const int warps = blockDim.x >> 5;
+
+    for (int g = blockIdx.x * warps + warp; g < n_work; g += gridDim.x * warps) {
+        const uint32_t item = work[g];
+        const h261b_session_dev_t &S = sessions[item >> 12];
+        const int mb = (int)(item & 0xFFFu);
+        const int mby = mb / S.mbw, mbx = mb - mby * S.mbw;
+        const bool do_me = (phases & H261B_PHASE_ME) && !S.skip_search;
+        const bool do_enc = (phases & H261B_PHASE_ENCDEC) != 0;
+        load_sources(s, S, mbx, mby, lane, do_me || do_enc);
+
+        me_gpu_mb_t me;
+        me.i_intra_cost = me.i_zero_cost = me.i_16x16_cost = me.i_16x16_filter_cost = 0;
+        me.s_16x16_mv.i8_mx = me.s_16x16_mv.i8_my = 0;
+        int8_t s1x = 0, s1y = 0;
+        if (do_me) {
+            motion_estimate(s, S, mbx, mby, lane, me, s1x, s1y);
+            if (lane == 0) {
+                if (S.me_out)
+                    S.me_out[mb] = me;
+                if (S.stage1_out) {
+                    S.stage1_out[mb].i8_mx = s1x;
+                    S.stage1_out[mb].i8_my = s1y;
+                }
+            }
+        }
+
+        MbDecision m;
+        if (phases & H261B_PHASE_MD) {
+            if (!do_me) {
+                /* intra picture without search: only the intra cost matters */
+                int32_t d[16];
+                const int sb = lane & 15;
+#pragma unroll
+                for (int k = 0; k < 16; k++)
+                    d[k] = cur_byte(s, (sb >> 2) * 4 + (k >> 2), (sb & 3) * 4 + (k & 3));
+                const int32_t v = satd4x4(d);
+                me.i_intra_cost = (int32_t)__reduce_add_sync(FULL, lane < 16 ? (uint32_t)v : 0u);
+            }
+            m = mode_decide(me, S.frame_type);
+            if (lane == 0 && S.md_out) {
+                h261_mb_mode_decision_t o;
+                o.i_cost = m.cost;
+                o.i_quantiser_adjust = 0;
+                o.i_mb_type = m.type;
+                o.i_mb_flags = m.flags;
+                o.i_mv_x = m.mvx;
+                o.i_mv_y = m.mvy;
+                S.md_out[mb] = o;
+            }
+        } else if (S.md_in) {
+            const h261_mb_mode_decision_t &d = S.md_in[mb];
+            m.type = d.i_mb_type;
+            m.flags = d.i_mb_flags;
+            m.mvx = d.i_mv_x;
+            m.mvy = d.i_mv_y;
+            m.cost = d.i_cost;
+        } else {
+            m.type = H261B_MB_TYPE_INTRA;
+            m.flags = m.mvx = m.mvy = m.cost = 0;
+        }
+
+        if (do_enc) {
+            int quant = S.quant;
+            if (S.md_in && !(phases & H261B_PHASE_MD))
+                quant += S.md_in[mb].i_quantiser_adjust;
+            quant = min(31, max(1, quant)); /* gpu_device.cu:625-627 */
+            int32_t stat[8];
+#pragma unroll
+            for (int v = 0; v < 8; v++)
+                stat[v] = 0;
+            uint32_t cbp = 0;
+            encdec_pass<FMAD>(s, S, mb, mbx, mby, m, quant, true, lane, stat, cbp);
+            encdec_pass<FMAD>(s, S, mb, mbx, mby, m, quant, false, lane, stat, cbp);
+
+            const int flags = m.flags | (cbp ? H261B_MB_COEFF : 0);
+            if (lane == 0) {
+                if (S.abi_out) {
+                    h261_macroblock_t *o = &S.abi_out[mb];
+                    o->i_macroblock_address = 0;
+                    o->i_macroblock_type = m.type;
+                    o->i_macroblock_type_flags = flags;
+                    o->i_macroblock_quant = quant;
+                    o->rgi_mv[0] = m.mvx;
+                    o->rgi_mv[1] = m.mvy;
+                    o->i_coded_block_pattern = (int32_t)cbp;
+                    o->i_mb_x = mbx * 16;
+                    o->i_mb_y = mby * 16;
+                }
+                if (S.info_out) {
+                    h261b_mb_info_t inf;
+                    inf.type = (int16_t)m.type;
+                    inf.flags = (int16_t)flags;
+                    inf.quant = (int8_t)quant;
+                    inf.cbp = (int8_t)cbp;
+                    inf.mvx = (int8_t)m.mvx;
+                    inf.mvy = (int8_t)m.mvy;
+                    inf.cost = m.cost;
+                    inf.reserved = 0;
+                    S.info_out[mb] = inf;
+                }
+            }
+            /* publish this MB's denoise statistics, then take a ticket */
+            h261b_denoise_dev_t *dn = S.dn;
+            const int t = m.type == H261B_MB_TYPE_INTRA ? 0 : 1;
+            if (lane < 8) {
+#pragma unroll
+                for (int v = 0; v < 8; v++)
+                    atomicAdd(&dn->noise[t][v * 8 + lane], stat[v]);
+            }
+            if (lane == 0)
+                atomicAdd(&dn->count[t], 6);
+            __threadfence();
+            __syncwarp();
+            uint32_t last = 0;
+            if (lane == 0)
+                last = atomicAdd(&dn->ticket, 1u) == (uint32_t)(S.mbw * S.mbh - 1) ? 1u : 0u;
+            last = __shfl_sync(FULL, last, 0);
+            if (last) {
+                __threadfence();
+                denoise_frame_end(dn, lane);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+} // namespace
+
+extern "C" int h261b_set_quant_table(void)
+{
+    /* f_inv_quant = 1.0 / ( float ) ( i_quant * 2 ) (mbgpu_kernels.cuh:685),
+     * evaluated on the host in IEEE double and rounded to float */
+    float tab[32];
+    tab[0] = 0.0f;
+    for (int q = 1; q < 32; q++)
+        tab[q] = (float)(1.0 / (double)(float)(q * 2));
+    return (int)cudaMemcpyToSymbol(c_inv_quant, tab, sizeof(tab));
+}
+
+extern "C" int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const uint32_t *work_dev,
+                                 int32_t n_work, int32_t phases, int32_t warps_per_cta, int32_t max_ctas,
+                                 void *stream)
+{
+    if (n_work <= 0)
+        return 0;
+    if (warps_per_cta < 1 || warps_per_cta > 8)
+        return (int)cudaErrorInvalidValue;
+    const int threads = warps_per_cta * 32;
+    const size_t smem = sizeof(WarpSmem) * (size_t)warps_per_cta;
+    int ctas = (n_work + warps_per_cta - 1) / warps_per_cta;
+    if (max_ctas > 0 && ctas > max_ctas)
+        ctas = max_ctas;
+    const int fmad = (phases >> 8) & 1;
+    const int ph = phases & 0xFF;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (fmad)
+        step_kernel<1><<<ctas, threads, smem, st>>>(sessions_dev, work_dev, n_work, ph);
+    else
+        step_kernel<0><<<ctas, threads, smem, st>>>(sessions_dev, work_dev, n_work, ph);
+    return (int)cudaGetLastError();
+}
+
+/* ------------------------------------------------ SAD primitive peak */
+
+namespace {
+
+/* the motion search's inner step, on registers: one funnel shift and one
+ * 4-pixel SAD per word, eight independent chains per thread */
+__global__ void __launch_bounds__(256) sad_peak_kernel(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
+                                                       int iters)
+{
+    uint32_t c[8], r[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        c[i] = in[(threadIdx.x + i) & 255];
+        r[i] = in[(threadIdx.x * 7 + i) & 255];
+    }
+    uint32_t acc = 0;
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            acc = sad4(c[i], r[i], acc);
+            r[i] = __funnelshift_r(r[i], r[(i + 1) & 7], 8);
+        }
+    }
+    out[blockIdx.x * blockDim.x + threadIdx.x] = acc;
+}
+
+} // namespace
+
+extern "C" int h261b_measure_sad_peak(int32_t device, double *absdiff_per_s)
+{
+    if (!absdiff_per_s)
+        return -1;
+    int sms = 0;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+        return -2;
+    const int blocks = sms * 8, threads = 256, iters = 2048;
+    uint32_t *in = nullptr, *out = nullptr;
+    uint32_t h[256];
+    for (int i = 0; i < 256; i++)
+        h[i] = (uint32_t)i * 2654435761u;
+    cudaEvent_t a, b;
+    float ms = 0.f;
+    int rc = -2;
+    if (cudaMalloc(&in, sizeof(h)) == cudaSuccess && cudaMalloc(&out, sizeof(uint32_t) * blocks * threads) == cudaSuccess &&
+        cudaMemcpy(in, h, sizeof(h), cudaMemcpyHostToDevice) == cudaSuccess && cudaEventCreate(&a) == cudaSuccess &&
+        cudaEventCreate(&b) == cudaSuccess) {
+        sad_peak_kernel<<<blocks, threads>>>(in, out, 64);
+        cudaEventRecord(a);
+        sad_peak_kernel<<<blocks, threads>>>(in, out, iters);
+        cudaEventRecord(b);
+        if (cudaEventSynchronize(b) == cudaSuccess && cudaEventElapsedTime(&ms, a, b) == cudaSuccess && ms > 0.f) {
+            *absdiff_per_s = (double)blocks * threads * iters * 8 * 4 / (ms * 1e-3);
+            rc = 0;
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+    cudaFree(in);
+    cudaFree(out);
+    return rc;
+}

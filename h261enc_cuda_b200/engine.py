@@ -1,0 +1,149 @@
+"""Batched encode engine (include/h261b.h) from Python.
+
+One ``Engine`` owns a CUDA stream, a device pool and the double-buffered
+upload / result arenas.  Sessions are independent encode streams; each
+``step()`` encodes the queued picture of every session in one launch.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+
+@dataclass
+class FrameResult:
+    frame_index: int
+    frame_type: int
+    quant: int
+    mbs: np.ndarray        # RESULT_DTYPE[num_mb]
+    levels: np.ndarray     # int8 [num_mb, 6, 64]
+
+    def to_abi(self, width: int) -> np.ndarray:
+        """The reference's h261_macroblock_t array for this picture."""
+        out = np.zeros(self.mbs.size, _lib.MB_DTYPE)
+        out["type"] = self.mbs["type"]
+        out["flags"] = self.mbs["flags"]
+        out["quant"] = self.mbs["quant"]
+        out["mv"][:, 0] = self.mbs["mvx"]
+        out["mv"][:, 1] = self.mbs["mvy"]
+        out["cbp"] = self.mbs["cbp"].astype(np.uint8)
+        tc = self.levels.astype(np.int32)
+        intra = self.mbs["type"] == _lib.MB_TYPE_INTRA
+        tc[intra, :, 0] = self.levels[intra, :, 0].view(np.uint8)
+        out["tcoeff"] = tc
+        mbw = width // 16
+        idx = np.arange(self.mbs.size)
+        out["mb_x"] = (idx % mbw) * 16
+        out["mb_y"] = (idx // mbw) * 16
+        return out
+
+
+class Engine:
+    def __init__(self, device: int = 0, max_sessions: int = 4096, hbm_budget_bytes: int = 0,
+                 me_mode: int = 0, fmad: int = 1, warps_per_cta: int = 0, max_ctas: int = 0):
+        lib = _lib.core()
+        cfg = _lib.EngineConfig()
+        lib.h261b_engine_config_default(ctypes.byref(cfg))
+        cfg.device, cfg.max_sessions, cfg.hbm_budget_bytes = device, max_sessions, hbm_budget_bytes
+        cfg.me_mode, cfg.fmad, cfg.warps_per_cta, cfg.max_ctas = me_mode, fmad, warps_per_cta, max_ctas
+        h = ctypes.c_void_p()
+        check(lib.h261b_engine_create(ctypes.byref(cfg), ctypes.byref(h)), "h261b_engine_create")
+        self._h = h
+        self._dims = {}
+
+    # -- sessions
+    def open(self, width: int, height: int, quant: int, intra_period: int = 0, denoise: int = 5) -> int:
+        c = _lib.SessionConfig(width, height, quant, intra_period, denoise)
+        sid = ctypes.c_int32()
+        check(_lib.core().h261b_session_open(self._h, ctypes.byref(c), ctypes.byref(sid)), "h261b_session_open")
+        self._dims[sid.value] = (width, height)
+        return sid.value
+
+    def close(self, sid: int) -> None:
+        check(_lib.core().h261b_session_close(self._h, sid), "h261b_session_close")
+        self._dims.pop(sid, None)
+
+    def submit(self, sid: int, y: np.ndarray, cb: np.ndarray, cr: np.ndarray, quant: int = 0) -> None:
+        check(_lib.core().h261b_session_submit(self._h, sid, _lib.ptr(y), _lib.ptr(cb), _lib.ptr(cr), quant),
+              "h261b_session_submit")
+
+    def submit_device(self, sid: int, y_ptr: int, cb_ptr: int, cr_ptr: int, quant: int = 0) -> None:
+        """Queue a picture already in device memory (raw device pointers)."""
+        check(_lib.core().h261b_session_submit_device(self._h, sid, ctypes.c_void_p(y_ptr), ctypes.c_void_p(cb_ptr),
+                                                      ctypes.c_void_p(cr_ptr), quant), "h261b_session_submit_device")
+
+    def submit_frame(self, sid: int, frame: np.ndarray, quant: int = 0) -> None:
+        w, h = self._dims[sid]
+        fs = w * h
+        self.submit(sid, frame[:fs], frame[fs:fs + fs // 4], frame[fs + fs // 4:fs + fs // 2], quant)
+
+    # -- steps
+    def step(self) -> int:
+        return check(_lib.core().h261b_engine_step(self._h), "h261b_engine_step")
+
+    def sync(self) -> None:
+        check(_lib.core().h261b_engine_sync(self._h), "h261b_engine_sync")
+
+    def result(self, sid: int, copy: bool = True) -> FrameResult:
+        r = _lib.FrameResult()
+        check(_lib.core().h261b_session_result(self._h, sid, ctypes.byref(r)), "h261b_session_result")
+        n = r.num_mb
+        mbs = np.ctypeslib.as_array((ctypes.c_uint8 * (n * 16)).from_address(r.mbs)).view(_lib.RESULT_DTYPE)
+        lv = np.ctypeslib.as_array(r.levels, shape=(n * 384,)).reshape(n, 6, 64)
+        if copy:
+            mbs, lv = mbs.copy(), lv.copy()
+        return FrameResult(r.frame_index, r.frame_type, r.quant, mbs, lv)
+
+    def recon(self, sid: int):
+        w, h = self._dims[sid]
+        y = np.empty(w * h, np.uint8)
+        cb = np.empty(w * h // 4, np.uint8)
+        cr = np.empty(w * h // 4, np.uint8)
+        check(_lib.core().h261b_session_recon(self._h, sid, _lib.ptr(y), _lib.ptr(cb), _lib.ptr(cr)),
+              "h261b_session_recon")
+        return y, cb, cr
+
+    def last_kernel_ms(self) -> float:
+        ms = ctypes.c_float()
+        check(_lib.core().h261b_engine_last_kernel_ms(self._h, ctypes.byref(ms)), "h261b_engine_last_kernel_ms")
+        return ms.value
+
+    def stats(self):
+        o, q, b = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()
+        check(_lib.core().h261b_engine_stats(self._h, ctypes.byref(o), ctypes.byref(q), ctypes.byref(b)),
+              "h261b_engine_stats")
+        return o.value, q.value, b.value
+
+    def destroy(self) -> None:
+        if self._h:
+            _lib.core().h261b_engine_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.destroy()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def session_bytes(width: int, height: int) -> int:
+    return int(_lib.core().h261b_session_bytes(width, height))
+
+
+def sad_peak(device: int = 0) -> float:
+    """Measured 4-pixel SAD throughput of the device, absolute differences/s."""
+    v = ctypes.c_double()
+    if _lib.core().h261b_measure_sad_peak(device, ctypes.byref(v)) != 0:
+        raise _lib.H261Error("h261b_measure_sad_peak failed")
+    return v.value

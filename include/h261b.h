@@ -1,0 +1,141 @@
+/*
+ * h261b.h -- native API of the B200 H.261 encode core (libh261b.so).
+ *
+ * Two ways in:
+ *   1. the reference's own boundary, h261b_abi.h (sixteen gpu_device.h entry
+ *      points, one process-global encoder, synchronous calls);
+ *   2. this batched engine: many independent encode sessions of mixed size
+ *      and QUANT share one device; each h261b_engine_step() encodes the next
+ *      picture of every session that has one queued, in one launch (one CUDA
+ *      graph replay) over a flat macroblock work list.  Source pictures go up
+ *      in one host-to-device copy per step, compact results come back in one
+ *      copy, reconstructions stay in HBM as the next reference.
+ *
+ * All functions return H261B_OK (0) or a negative status; the text of the
+ * last failure on the calling thread is available from h261b_last_error().
+ * Nothing here takes or returns framework types: plain pointers and sizes.
+ * An engine is used from one host thread at a time.
+ */
+#ifndef H261B_H
+#define H261B_H
+
+#include <stdint.h>
+#include "h261b_abi.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define H261B_OK              0
+#define H261B_ERR_ARG        -1   /* bad argument or unsupported size       */
+#define H261B_ERR_CUDA       -2   /* CUDA runtime error (message has it)    */
+#define H261B_ERR_NOMEM      -3   /* host or device allocation failed       */
+#define H261B_ERR_BUDGET     -4   /* admission refused: HBM budget exceeded */
+#define H261B_ERR_STATE      -5   /* call out of order                      */
+#define H261B_ERR_NO_DEVICE  -6   /* no CUDA device / library not usable    */
+
+#define H261B_ME_REFERENCE 0      /* the reference's two-stage search       */
+#define H261B_ME_FULL      1      /* exhaustive +-15 (not bit-exact to it)  */
+
+/* text of the last error on this thread ("" if none) */
+const char *h261b_last_error(void);
+/* last status recorded by a call of the reference-compatible boundary */
+int h261b_abi_last_status(void);
+/* library version string */
+const char *h261b_version(void);
+
+typedef struct h261b_engine_s h261b_engine_t;
+
+typedef struct {
+    int32_t device;           /* CUDA device ordinal                         */
+    int32_t max_sessions;     /* session slots (<= 65536)                    */
+    int64_t hbm_budget_bytes; /* admission limit for session pictures, 0 = none */
+    int32_t me_mode;          /* H261B_ME_REFERENCE / H261B_ME_FULL          */
+    int32_t fmad;             /* 1: fused double multiply-add in the DCTs
+                                 (bit-exact to the reference built with nvcc
+                                 defaults), 0: separately rounded            */
+    int32_t warps_per_cta;    /* 1..8, 0 = tuned                              */
+    int32_t max_ctas;         /* grid cap, 0 = one wave of resident CTAs     */
+    int32_t use_graphs;       /* 1: replay each step from a CUDA graph       */
+} h261b_engine_config_t;
+
+void h261b_engine_config_default(h261b_engine_config_t *cfg);
+int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engine_t **out);
+int h261b_engine_destroy(h261b_engine_t *e);
+
+typedef struct {
+    int32_t width, height;    /* multiples of 16, e.g. 176x144 or 352x288    */
+    int32_t quant;            /* fixed picture QUANT 1..31                   */
+    int32_t intra_period;     /* 0: only the first picture is intra          */
+    int32_t denoise;          /* DCT-domain denoise strength (reference: 5)  */
+} h261b_session_config_t;
+
+/* Device bytes one session of this size holds (pictures + state). */
+int64_t h261b_session_bytes(int32_t width, int32_t height);
+
+int h261b_session_open(h261b_engine_t *e, const h261b_session_config_t *cfg, int32_t *session_id);
+int h261b_session_close(h261b_engine_t *e, int32_t session_id);
+
+/* Queue the session's next source picture (packed planes: Y stride W,
+ * chroma stride W/2); the bytes are copied before the call returns.
+ * quant > 0 replaces the session's QUANT from this picture on. */
+int h261b_session_submit(h261b_engine_t *e, int32_t session_id, const uint8_t *y, const uint8_t *cb,
+                         const uint8_t *cr, int32_t quant);
+
+/* Queue a picture that is already in device memory (packed planes, pitch W
+ * and W/2; Y 16-byte and Cb/Cr 8-byte aligned).  It must stay unchanged
+ * until the step that reads it has completed. */
+int h261b_session_submit_device(h261b_engine_t *e, int32_t session_id, const uint8_t *y, const uint8_t *cb,
+                                const uint8_t *cr, int32_t quant);
+
+/* Encode the queued picture of every session that has one (one frame-step).
+ * Returns the number of pictures encoded (>= 0) or a negative status.  The
+ * call is asynchronous; results become readable after h261b_engine_sync(). */
+int h261b_engine_step(h261b_engine_t *e);
+int h261b_engine_sync(h261b_engine_t *e);
+
+/* per-macroblock result of a step (16 bytes) */
+typedef struct {
+    int16_t type;             /* 0 intra, 2 inter                             */
+    int16_t flags;            /* 1 MC | 2 FILTER | 4 COEFF                    */
+    int8_t quant;
+    int8_t cbp;               /* bit 32>>b set when block b is coded          */
+    int8_t mvx, mvy;
+    int32_t cost;             /* mode-decision SATD cost                      */
+    int32_t reserved;
+} h261b_mb_result_t;
+
+typedef struct {
+    int32_t frame_index;      /* picture number within the session           */
+    int32_t frame_type;       /* 0 intra, 1 inter                             */
+    int32_t quant;            /* picture QUANT used                           */
+    int32_t num_mb;
+    const h261b_mb_result_t *mbs;  /* num_mb entries                          */
+    const int8_t *levels;     /* num_mb x 6 x 64 quantised levels, raster
+                                 order; an intra DC is stored as uint8 1..255 */
+} h261b_frame_result_t;
+
+/* Results of the last completed step for a session (pointers stay valid
+ * until the next h261b_engine_step()). Requires h261b_engine_sync(). */
+int h261b_session_result(h261b_engine_t *e, int32_t session_id, h261b_frame_result_t *out);
+
+/* Copy the session's latest reconstruction (packed planes) to the host. */
+int h261b_session_recon(h261b_engine_t *e, int32_t session_id, uint8_t *y, uint8_t *cb, uint8_t *cr);
+
+/* Expand one result into the reference's h261_macroblock_t array (what the
+ * reference's GOB / macroblock writers read); mbs[] gets num_mb entries. */
+int h261b_result_to_abi(const h261b_frame_result_t *r, int32_t width, h261_macroblock_t *mbs);
+
+/* Device time of the last step's kernel in milliseconds (CUDA events). */
+int h261b_engine_last_kernel_ms(h261b_engine_t *e, float *ms);
+/* Throughput of the 4-pixel SAD primitive the motion search uses, measured
+ * on the device with every SM busy: absolute differences per second. */
+int h261b_measure_sad_peak(int32_t device, double *absdiff_per_s);
+
+/* Number of sessions open / queued, device bytes held. */
+int h261b_engine_stats(h261b_engine_t *e, int32_t *open_sessions, int32_t *queued, int64_t *device_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

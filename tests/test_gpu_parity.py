@@ -1,0 +1,154 @@
+"""GPU parity of the sm_100a core against the CPU oracle: bit-exact motion
+vectors, costs, MB types and flags, CBP, quantised levels and
+reconstructions, through the batched engine and through the reference's own
+boundary (the sixteen gpu_device.h calls)."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import oracle as O
+from h261enc_cuda_b200 import synth
+from h261enc_cuda_b200.compat import Boundary
+from h261enc_cuda_b200.engine import Engine
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("type", "flags", "quant", "cbp")
+
+
+def assert_mbs_equal(got, want, where):
+    for f in FIELDS:
+        bad = np.nonzero(got[f] != want[f])[0]
+        assert bad.size == 0, f"{where}: field {f} differs at MBs {bad[:8].tolist()}"
+    assert np.array_equal(got["mv"], want["mv"]), f"{where}: motion vectors differ"
+    bad = np.nonzero((got["tcoeff"] != want["tcoeff"]).any(axis=(1, 2)))[0]
+    assert bad.size == 0, f"{where}: levels differ at MBs {bad[:8].tolist()}"
+
+
+def run_engine(frames, w, h, quant, intra=0, me_mode=0, warps=4, fmad=1):
+    out_mbs, out_rec = [], []
+    with Engine(me_mode=me_mode, warps_per_cta=warps, fmad=fmad) as e:
+        sid = e.open(w, h, quant, intra_period=intra)
+        for i in range(frames.shape[0]):
+            e.submit_frame(sid, frames[i])
+            assert e.step() == 1
+            e.sync()
+            r = e.result(sid)
+            assert r.frame_index == i
+            out_mbs.append(r.to_abi(w))
+            out_rec.append(np.concatenate(e.recon(sid)))
+    return out_mbs, np.stack(out_rec)
+
+
+@pytest.mark.parametrize("preset,w,h,n,quant,intra,me_mode", [
+    (0, 176, 144, 30, 8, 0, 0),      # config 0: QCIF, I then P, QUANT 8
+    (1, 352, 288, 8, 12, 4, 0),      # CIF objects, intra every 4 pictures
+    (0, 176, 144, 6, 1, 0, 0),       # finest quantiser: many large levels
+    (0, 176, 144, 6, 31, 0, 0),      # coarsest quantiser
+    (3, 176, 144, 8, 12, 0, 0),      # config 3 content: random block motion
+    (0, 176, 144, 5, 8, 0, 1),       # exhaustive +-15 search extension
+])
+def test_engine_matches_oracle(gpu, preset, w, h, n, quant, intra, me_mode):
+    fr = synth.clip(preset, w, h, 1 + preset, n)
+    want = O.encode_sequence(fr, w, h, quant, intra_period=intra, me_mode=me_mode)
+    got_mbs, got_rec = run_engine(fr, w, h, quant, intra=intra, me_mode=me_mode)
+    for i in range(n):
+        assert_mbs_equal(got_mbs[i], want["mbs"][i], f"frame {i}")
+        assert np.array_equal(got_rec[i], want["recon"][i]), f"frame {i}: reconstruction differs"
+
+
+@pytest.mark.parametrize("warps", [1, 2, 8])
+def test_launch_shape_does_not_change_output(gpu, warps):
+    fr = synth.clip(0, 176, 144, 9, 4)
+    a, ra = run_engine(fr, 176, 144, 8, warps=warps)
+    b, rb = run_engine(fr, 176, 144, 8, warps=4)
+    assert np.array_equal(ra, rb)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+
+
+def test_batch_equals_alone_with_joins(gpu):
+    """Sessions of mixed size and QUANT that share steps, joining at
+    different times, produce exactly what each produces alone (and what the
+    oracle produces)."""
+    specs = [(176, 144, 8, 0, 11), (352, 288, 12, 0, 12), (176, 144, 4, 3, 13), (352, 288, 20, 0, 14),
+             (176, 144, 24, 0, 15), (176, 144, 6, 0, 16)]
+    n = 6
+    clips = [synth.clip(2, w, h, seed, n) for (w, h, q, start, seed) in specs]
+    want = [O.encode_sequence(c, w, h, q) for c, (w, h, q, s, _) in zip(clips, specs)]
+    got = [[] for _ in specs]
+    with Engine(warps_per_cta=4) as e:
+        sids = [None] * len(specs)
+        for t in range(n + 3):
+            for k, (w, h, q, start, _) in enumerate(specs):
+                i = t - start
+                if i == 0:
+                    sids[k] = e.open(w, h, q)
+                if 0 <= i < n:
+                    e.submit_frame(sids[k], clips[k][i])
+            e.step()
+            e.sync()
+            for k, (w, h, q, start, _) in enumerate(specs):
+                i = t - start
+                if 0 <= i < n:
+                    got[k].append((e.result(sids[k]).to_abi(w), np.concatenate(e.recon(sids[k]))))
+    for k, (w, h, q, start, _) in enumerate(specs):
+        assert len(got[k]) == n
+        for i in range(n):
+            assert_mbs_equal(got[k][i][0], want[k]["mbs"][i], f"session {k} frame {i}")
+            assert np.array_equal(got[k][i][1], want[k]["recon"][i])
+
+
+def test_boundary_matches_oracle(gpu):
+    """The sixteen reference entry points: ME results (costs and vectors),
+    encode with a host mode decision, decode."""
+    w, h, n = 176, 144, 8
+    fr = synth.clip(0, w, h, 21, n)
+    fs = w * h
+    b = Boundary(w, h, denoise=5)
+    try:
+        ref = np.zeros(fs * 3 // 2, np.uint8)
+        want = O.encode_sequence(fr, w, h, 8)
+        for i in range(n):
+            cur = fr[i]
+            b.set_current(cur[:fs], cur[fs:fs + fs // 4], cur[fs + fs // 4:])
+            b.set_reference(ref[:fs], ref[fs:fs + fs // 4], ref[fs + fs // 4:])
+            me = b.motion_estimation()
+            ome, _ = O.me_frame(cur[:fs], ref[:fs], w, h)
+            for f in ("intra", "cost", "fcost", "mvx", "mvy"):
+                assert np.array_equal(me[f], ome[f]), f"frame {i}: ME field {f}"
+            ft = 0 if i == 0 else 1
+            md = O.mode_decision(ome, ft)
+            mbs = b.encode(md, 8, ft)
+            assert_mbs_equal(mbs, want["mbs"][i], f"frame {i}")
+            y, cb, cr = b.decode()
+            ref = np.concatenate([y, cb, cr])
+            assert np.array_equal(ref, want["recon"][i])
+    finally:
+        b.close()
+
+
+needs_drivers = pytest.mark.skipif(not (os.path.exists(O.DRIVERS["ours"]) and os.path.exists(O.DRIVERS["oracle"])),
+                                   reason="frame-loop drivers not built")
+
+
+@needs_drivers
+@pytest.mark.parametrize("w,h,n,quant,intra,preset", [(176, 144, 12, 8, 0, 0), (352, 288, 6, 0, 132, 1)])
+def test_reference_host_code_on_our_core(gpu, w, h, n, quant, intra, preset):
+    """The reference's unchanged host code (mode decision, rate control,
+    writers) linked against libh261b.so writes the same bitstream, and
+    dumps the same boundary values, as on the CPU oracle."""
+    fr = synth.clip(preset, w, h, 31, n)
+    with tempfile.TemporaryDirectory() as td:
+        yuv = os.path.join(td, "in.yuv")
+        fr.tofile(yuv)
+        ob, orc, od = O.run_driver("oracle", yuv, w, h, n, td, quant=quant, intra=intra)
+        gb, grc, gd = O.run_driver("ours", yuv, w, h, n, td, quant=quant, intra=intra)
+        assert open(gb, "rb").read() == open(ob, "rb").read()
+        assert open(grc, "rb").read() == open(orc, "rb").read()
+        for a, c in zip(O.read_dump(gd), O.read_dump(od)):
+            assert a["quant"] == c["quant"] and a["bytes"] == c["bytes"]
+            assert np.array_equal(a["me"], c["me"]) and np.array_equal(a["md"], c["md"])
+            assert np.array_equal(a["mbs"], c["mbs"])
