@@ -43,11 +43,11 @@ def run_engine(frames, w, h, quant, intra=0, me_mode=0, warps=4, fmad=1):
 
 
 @pytest.mark.parametrize("preset,w,h,n,quant,intra,me_mode", [
-    (0, 176, 144, 30, 8, 0, 0),      # config 0: QCIF, I then P, QUANT 8
+    (0, 176, 144, 30, 8, 0, 0),      # QCIF pan + objects, I then P, QUANT 8
     (1, 352, 288, 8, 12, 4, 0),      # CIF objects, intra every 4 pictures
     (0, 176, 144, 6, 1, 0, 0),       # finest quantiser: many large levels
     (0, 176, 144, 6, 31, 0, 0),      # coarsest quantiser
-    (3, 176, 144, 8, 12, 0, 0),      # config 3 content: random block motion
+    (3, 176, 144, 8, 12, 0, 0),      # per-block random motion content
     (0, 176, 144, 5, 8, 0, 1),       # exhaustive +-15 search extension
 ])
 def test_engine_matches_oracle(gpu, preset, w, h, n, quant, intra, me_mode):
