@@ -14,7 +14,7 @@
 #define H261B_DEVICE_H
 
 #include <stdint.h>
-#include "../../include/h261b_abi.h"
+#include "../../include/h261b.h"
 
 #define H261B_MAX_MB_PER_SESSION 4096
 

@@ -132,6 +132,40 @@ int h261b_engine_last_kernel_ms(h261b_engine_t *e, float *ms);
  * on the device with every SM busy: absolute differences per second. */
 int h261b_measure_sad_peak(int32_t device, double *absdiff_per_s);
 
+/* ---- one picture, no allocation ------------------------------------------
+ * No counterpart in the reference: this entry point exists for callers that
+ * cannot call cudaMalloc (their device memory belongs to another allocator
+ * or pool, or an allocation is not allowed where they run).  The caller
+ * passes every input, output and state buffer as device memory; the small
+ * scratch the kernel needs (descriptor and work list) is a fixed static
+ * device array inside the library, so the call allocates nothing.  Limits:
+ * pictures of at most H261B_NOALLOC_MAX_MB macroblocks (larger ones are
+ * refused with H261B_ERR_ARG); the first call on a device sets up the
+ * scratch address and should come before any stream capture; calls whose
+ * work overlaps on the GPU race on the shared scratch (use one stream). */
+#define H261B_NOALLOC_MAX_MB      4096
+#define H261B_NOALLOC_STATE_BYTES 1040   /* per-stream denoise state          */
+
+typedef struct {
+    int32_t width, height;    /* multiples of 16                              */
+    int32_t frame_type;       /* H261B_FRAME_TYPE_INTRA / _INTER              */
+    int32_t quant;            /* picture QUANT 1..31                          */
+    int32_t me_mode;          /* H261B_ME_REFERENCE / H261B_ME_FULL           */
+    int32_t fmad;             /* 1: the reference's default-build arithmetic  */
+    int32_t denoise;          /* strength written when reset_state is set     */
+    int32_t reset_state;      /* 1: first picture of a stream, clear state    */
+    const uint8_t *cur_y, *cur_cb, *cur_cr;  /* device: source, pitch W / W/2 */
+    const uint8_t *ref_y, *ref_cb, *ref_cr;  /* device: previous reconstruction */
+    uint8_t *rec_y, *rec_cb, *rec_cr;        /* device: reconstruction (out)  */
+    void *state;              /* device: H261B_NOALLOC_STATE_BYTES, in/out     */
+    h261b_mb_result_t *mbs;   /* device: num_mb results (out)                 */
+    int8_t *levels;           /* device: num_mb x 384 levels (out)            */
+} h261b_noalloc_picture_t;
+
+/* Queue the encode of one picture on `stream` (a cudaStream_t, may be 0).
+ * Luma planes 16-byte aligned, chroma planes and state 8-byte aligned. */
+int h261b_encode_picture_noalloc(const h261b_noalloc_picture_t *pic, void *stream);
+
 /* Number of sessions open / queued, device bytes held. */
 int h261b_engine_stats(h261b_engine_t *e, int32_t *open_sessions, int32_t *queued, int64_t *device_bytes);
 
