@@ -12,11 +12,16 @@ h261enc_cuda_b200/workloads.py).
           write) before every timed step, the step kernel timed with CUDA
           events on the engine's stream;
   e2e     the same through the public API with host buffers: every step
-          copies its pictures from host memory into the pinned arena, moves
-          them to the device, encodes, and reads the compact results back;
+          copies the pictures of all streams from host memory into the
+          pinned staging arena (h261b_engine_submit_batch, the engine's copy
+          threads), moves them to the device, encodes, and copies records
+          and levels back; the host reads step k-1's records while step k
+          runs (two streams);
   single_stream  the same streams one at a time (one picture per step,
           synchronous), the plain single-stream path;
-  latency_ms     per-picture latency (submit -> results on the host).
+  latency_ms     per-picture latency: batched = submit of a step -> its
+          records read on the host (pipelined), single = one synchronous
+          picture.
 
 ``--impl reference`` times the CPU restatement of the reference's device
 path (oracle/) on all host cores instead.  Under torchrun every rank encodes
@@ -29,7 +34,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -54,7 +58,7 @@ SAD_PER_MB = 170 * 256
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=8)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batch64")
@@ -65,52 +69,72 @@ def parse():
 # --------------------------------------------------------------- helpers
 
 class ClockSampler:
-    """nvidia-smi samples (200 ms) while the timed region runs."""
+    """SM clock, power and clock-event reasons sampled through NVML every
+    5 ms while the timed region runs (the fields nvidia-smi's
+    clocks_event_reasons.* report)."""
 
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake_slowdown", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
 
-    def __init__(self, device: int):
-        self.device = device
-        self.proc = None
+    def __init__(self, device: int, period_s: float = 0.005):
+        self.device, self.period = device, period_s
+        self.samples, self.max_mhz, self.nv, self.h = [], None, None, None
+
+    def _handle(self):
+        import pynvml as nv
+        import torch
+        nv.nvmlInit()
+        props = torch.cuda.get_device_properties(self.device)
+        try:
+            return nv, nv.nvmlDeviceGetHandleByUUID("GPU-" + str(props.uuid))
+        except Exception:
+            bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
+            return nv, nv.nvmlDeviceGetHandleByPciBusId(bus)
+
+    def _run(self):
+        nv, h = self.nv, self.h
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                self.samples.append((sm, rs, pw))
+            except Exception:
+                pass
+            self.stop.wait(self.period)
 
     def __enter__(self):
+        self.stop = threading.Event()
+        self.thread = None
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except OSError:
-            self.proc = None
+            self.nv, self.h = self._handle()
+            self.max_mhz = self.nv.nvmlDeviceGetMaxClockInfo(self.h, self.nv.NVML_CLOCK_SM)
+            self.thread = threading.Thread(target=self._run, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.thread = None
         return self
 
     def __exit__(self, *exc):
-        self.out = ""
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.out, _ = self.proc.communicate(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-                self.out, _ = self.proc.communicate()
+        self.stop.set()
+        if self.thread:
+            self.thread.join()
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in (self.out or "").strip().splitlines():
-            p = [x.strip() for x in line.split(",")]
-            if len(p) < 8:
-                continue
-            try:
-                sm.append(float(p[0]))
-                mx = float(p[1])
-            except ValueError:
-                continue
-            for n, v in zip(names, p[4:8]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        import pynvml as nv
+        sm = [x[0] for x in self.samples]
+        reasons = set()
+        for _, rs, _ in self.samples:
+            for name, const in self.REASONS:
+                if rs & getattr(nv, const, 0):
+                    reasons.add(name)
+        pw = [x[2] for x in self.samples]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvml, 5 ms",
+                "power_w": statistics.median(pw) if pw else None}
 
 
 def hbm_peak():
@@ -220,26 +244,41 @@ def device_clips(streams, clip_len, device):
 
 class Runner:
     """Keeps the workload's slots full: a stream that reaches its length is
-    closed and a new session (same geometry and QUANT) takes the slot."""
+    closed and a new session (same geometry and QUANT) takes the slot.  The
+    engine returns a closed session's device slot to its pool once the
+    steps in flight that use it have completed, so nothing drains here."""
 
-    def __init__(self, engine, streams):
-        self.e, self.streams = engine, streams
+    def __init__(self, engine, streams, pools):
+        self.e, self.streams, self.pools = engine, streams, pools
         self.sids = [engine.open(s.width, s.height, s.quant) for s in streams]
         self.pos = [0] * len(streams)
+        # host pictures: one contiguous (clip, W*H*3/2) array per stream
+        self.base = np.array([p[1].ctypes.data for p in pools], np.uint64)
+        self.fbytes = np.array([p[1].shape[1] for p in pools], np.uint64)
+        self.ny = np.array([s.width * s.height for s in streams], np.uint64)
 
-    def queue(self, pools, on_device: bool):
+    def _advance(self):
         from h261enc_cuda_b200 import workloads
+        idx = np.empty(len(self.streams), np.uint64)
         for k, s in enumerate(self.streams):
             if self.pos[k] >= s.length:
                 self.e.close(self.sids[k])
                 self.sids[k] = self.e.open(s.width, s.height, s.quant)
                 self.pos[k] = 0
-            i = workloads.clip_index(self.pos[k], CLIP_LEN)
-            if on_device:
-                self.e.submit_device(self.sids[k], *pools[k][2][i])
-            else:
-                self.e.submit_frame(self.sids[k], pools[k][1][i])
+            idx[k] = workloads.clip_index(self.pos[k], CLIP_LEN)
             self.pos[k] += 1
+        return idx
+
+    def queue_device(self):
+        idx = self._advance()
+        for k, sid in enumerate(self.sids):
+            self.e.submit_device(sid, *self.pools[k][2][int(idx[k])])
+
+    def queue_host(self):
+        """The next picture of every stream from host memory, in one call."""
+        idx = self._advance()
+        y = self.base + idx * self.fbytes
+        self.e.submit_batch(self.sids, y, y + self.ny, y + self.ny + self.ny // 4)
 
 
 def ours(args, world, rank, local, dist):
@@ -255,10 +294,10 @@ def ours(args, world, rank, local, dist):
     peak_sad = sad_peak(local)
 
     eng = Engine(device=local, max_sessions=4 * len(streams))
-    run = Runner(eng, streams)
-    # warm-up (includes the launch-shape tuning steps)
-    for _ in range(max(args.warmup, 8)):
-        run.queue(pools, True)
+    run = Runner(eng, streams, pools)
+    # warm-up (includes the launch-shape tuning steps), both input paths
+    for i in range(max(args.warmup, 8)):
+        run.queue_device() if i % 2 else run.queue_host()
         eng.step()
         eng.sync()
 
@@ -271,7 +310,7 @@ def ours(args, world, rank, local, dist):
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
-            run.queue(pools, True)
+            run.queue_device()
             eng.step()
             kernel_ms.append(eng.last_kernel_ms())
         eng.sync()
@@ -283,23 +322,31 @@ def ours(args, world, rank, local, dist):
         total_ms = float(t.item())
     value = mb_per_step * args.steps * world / (total_ms * 1e-3)
 
-    # ---- e2e: host pictures through the public API, results read back
-    h2d = sum(s.width * s.height * 3 // 2 for s in streams)
-    d2h = sum(s.num_mb * (16 + 384) for s in streams)
-    lat = []
+    # ---- e2e: host pictures through the public API, results read back.
+    # Step k is issued, then the host waits for step k-1 and reads its MB
+    # records while step k runs (the engine alternates two streams).
+    chk = np.uint64(0)
+    lat, issued = [], []
+    h2d = d2h = 0
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        ts = time.perf_counter()
-        run.queue(pools, False)
+    for it in range(args.steps):
+        issued.append(time.perf_counter())
+        run.queue_host()
         eng.step()
-        eng.sync()
-        chk = 0
-        for sid in run.sids[:1]:
-            chk += int(eng.result(sid, copy=False).mbs["cost"].sum())
-        lat.append((time.perf_counter() - ts) * 1e3)
+        b_in, b_out = eng.last_copy_bytes()
+        h2d, d2h = h2d + b_in, d2h + b_out
+        if it > 0:
+            eng.wait_previous()
+            _, recs = eng.step_records()
+            chk ^= np.bitwise_xor.reduce(recs.view(np.uint64))
+            lat.append((time.perf_counter() - issued[it - 1]) * 1e3)
+    eng.sync()
+    _, recs = eng.step_records()
+    chk ^= np.bitwise_xor.reduce(recs.view(np.uint64))
+    lat.append((time.perf_counter() - issued[-1]) * 1e3)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     if dist:
@@ -307,6 +354,8 @@ def ours(args, world, rank, local, dist):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
     e2e = mb_per_step * args.steps * world / e2e_s
+    h2d //= args.steps
+    d2h //= args.steps
     eng.destroy()
 
     # ---- single stream: the same streams one at a time, one picture per step
@@ -348,7 +397,9 @@ def ours(args, world, rank, local, dist):
         "config": {"workload": args.workload, "streams": len(streams), "mb_per_step": mb_per_step,
                    "me_mode": "reference (11x11 grid + 7x7 refinement)",
                    "l2": "flushed before every timed step (256 MiB write)", "parallelism": f"sessions x{world}"},
-        "e2e": {"value": e2e, "unit": "MB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "e2e": {"value": e2e, "unit": "MB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "host_input": "pageable numpy clips -> pinned arena -> HBM, every step",
+                "l2": "not flushed (steady pipeline: inputs arrive from the host each step)"},
         "single_stream": {"value": single, "unit": "MB/s", "pictures": len(single_lat)},
         "batch_vs_single": value / single,
         "latency_ms": {"batched_p50": float(np.percentile(lat, 50)), "batched_p99": float(np.percentile(lat, 99)),

@@ -61,7 +61,7 @@ assert RESULT_DTYPE.itemsize == 16
 class EngineConfig(Structure):
     _fields_ = [("device", c_int32), ("max_sessions", c_int32), ("hbm_budget_bytes", c_int64),
                 ("me_mode", c_int32), ("fmad", c_int32), ("warps_per_cta", c_int32),
-                ("max_ctas", c_int32), ("use_graphs", c_int32)]
+                ("max_ctas", c_int32), ("copy_threads", c_int32)]
 
 
 class SessionConfig(Structure):
@@ -111,8 +111,17 @@ def core() -> ctypes.CDLL:
         lib.h261b_session_submit.argtypes = [c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_int32]
         lib.h261b_session_submit_device.argtypes = [c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_int32]
         lib.h261b_measure_sad_peak.argtypes = [c_int32, POINTER(ctypes.c_double)]
+        lib.h261b_session_input.argtypes = [c_void_p, c_int32, c_int32, POINTER(POINTER(c_uint8)),
+                                            POINTER(POINTER(c_uint8)), POINTER(POINTER(c_uint8))]
+        lib.h261b_engine_submit_batch.argtypes = [c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
+                                                  c_void_p]
+        lib.h261b_engine_last_copy_bytes.argtypes = [c_void_p, POINTER(ctypes.c_int64), POINTER(ctypes.c_int64)]
+        lib.h261b_engine_inputs.argtypes = [c_void_p, c_int32, c_void_p, c_void_p, POINTER(c_void_p), c_void_p]
+        lib.h261b_engine_step_records.argtypes = [c_void_p, POINTER(c_void_p), POINTER(ctypes.c_int64),
+                                                  POINTER(ctypes.c_int64)]
         lib.h261b_engine_step.argtypes = [c_void_p]
         lib.h261b_engine_sync.argtypes = [c_void_p]
+        lib.h261b_engine_wait_previous.argtypes = [c_void_p]
         lib.h261b_session_result.argtypes = [c_void_p, c_int32, POINTER(FrameResult)]
         lib.h261b_session_recon.argtypes = [c_void_p, c_int32, c_void_p, c_void_p, c_void_p]
         lib.h261b_result_to_abi.argtypes = [POINTER(FrameResult), c_int32, c_void_p]

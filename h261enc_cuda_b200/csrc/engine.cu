@@ -4,12 +4,18 @@
  * Memory: every open session owns two reconstruction pictures in HBM (they
  * alternate as reference and output) and its denoise state, taken from a
  * size-class slab pool so that opening a session in steady state does not
- * call cudaMalloc.  Queued source pictures are packed by h261b_session_submit
- * into a pinned upload arena; a step moves the whole arena with one copy,
- * runs one launch over the flat (session, MB) work list, and brings the
- * compact results of all sessions back with one copy.  Arenas, descriptors
- * and results are double-buffered by step parity, so the host can queue the
- * next step and read the previous results while a step runs.
+ * call cudaMalloc.  Queued source pictures sit in a pinned upload arena
+ * (copied there by h261b_session_submit, or written there directly by the
+ * caller through h261b_session_input); a step moves the whole arena with
+ * one copy, runs one launch over the flat (session, MB) work list, and
+ * brings the compact results of all sessions back with one copy.
+ *
+ * Pipelining: steps alternate between two CUDA streams and two sets of
+ * arenas (by step parity).  Within a step the order is upload -> kernel ->
+ * download; across steps only the kernels are ordered (step k+1's kernel
+ * waits for step k's, whose reconstructions are its references), so step
+ * k+1's upload overlaps step k's kernel and step k's download overlaps step
+ * k+1's kernel.  Results of step k stay readable until step k+2 is issued.
  *
  * Tuning: when warps_per_cta is 0 the first steps try each launch shape on
  * live work (the results do not depend on it) and keep the fastest by CUDA
@@ -20,11 +26,12 @@
 #include <algorithm>
 #include <cstring>
 #include <map>
-#include <mutex>
-#include <string>
+#include <memory>
+#include <thread>
 #include <vector>
 
 #include "common.h"
+#include "copy_pool.h"
 #include "h261b_device.h"
 
 namespace h261b {
@@ -122,6 +129,13 @@ struct Mirror {
     }
 };
 
+/* where one step left a session's results */
+struct Result {
+    int64_t step = -1;
+    int32_t frame = 0, type = 0, quant = 0;
+    size_t info_off = 0, level_off = 0;
+};
+
 struct Session {
     bool open = false;
     int32_t w = 0, h = 0, mbw = 0, mbh = 0, nmb = 0;
@@ -137,11 +151,7 @@ struct Session {
     size_t src_off = 0;
     const uint8_t *dev_src[3] = { nullptr, nullptr, nullptr };
     int32_t queued_quant = 0;
-    /* last completed step */
-    bool has_result = false;
-    int res_parity = 0;
-    size_t info_off = 0, level_off = 0;
-    int32_t res_frame = 0, res_type = 0, res_quant = 0;
+    Result res[2];                 /* by step parity                      */
 };
 
 } // namespace h261b
@@ -151,7 +161,7 @@ using namespace h261b;
 struct h261b_engine_s {
     h261b_engine_config_t cfg;
     int sm_count = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream[2] = { nullptr, nullptr };
     DevicePool pool;
     std::vector<Session> sessions;
     int32_t open_count = 0;
@@ -160,15 +170,27 @@ struct h261b_engine_s {
     Mirror upload[2];          /* queued source pictures                  */
     Mirror results[2];         /* mb info + levels of every session        */
     Mirror desc[2];            /* session descriptors + work list           */
-    size_t upload_used = 0;    /* bytes queued into upload[parity]         */
-    int parity = 0;            /* arena the next step uses                 */
-    cudaEvent_t h2d_done[2] = { nullptr, nullptr };
-    cudaEvent_t step_done[2] = { nullptr, nullptr };
-    cudaEvent_t k_start = nullptr, k_end = nullptr;
+    size_t upload_used = 0;    /* bytes queued for the next step           */
     bool upload_checked = false;
+    int64_t next_step = 0;     /* id of the next step; parity = id & 1      */
+    int64_t done_step = -1;    /* every step up to this one has completed   */
+    cudaEvent_t h2d_done[2] = { nullptr, nullptr };
+    cudaEvent_t kernel_done[2] = { nullptr, nullptr };
+    cudaEvent_t step_done[2] = { nullptr, nullptr };
+    cudaEvent_t k_start[2] = { nullptr, nullptr }, k_end[2] = { nullptr, nullptr };
     bool in_flight[2] = { false, false };
-    int last_parity = -1;
-    std::vector<int32_t> last_stepped;
+    int64_t step_mbs[2] = { 0, 0 };   /* MB records of the step in each arena */
+    int64_t last_h2d = 0, last_d2h = 0;  /* bytes copied by the last step */
+    /* slots of closed sessions, returned to the pool once the last step
+     * that may use them (second field) has completed */
+    struct Retired {
+        void *block;
+        size_t bytes;
+        int64_t last_step;
+    };
+    std::vector<Retired> retired;
+    std::unique_ptr<CopyPool> copier;   /* batched submissions */
+    std::vector<CopyJob> copy_jobs;
 
     /* launch tuning */
     int warps = 4, ctas = 0;
@@ -178,7 +200,7 @@ struct h261b_engine_s {
     bool tuned = false;
 };
 
-static const char *k_version = "h261b 0.1 (sm_100a)";
+static const char *k_version = "h261b 0.2 (sm_100a)";
 
 extern "C" const char *h261b_last_error(void) { return g_err; }
 extern "C" const char *h261b_version(void) { return k_version; }
@@ -193,7 +215,7 @@ extern "C" void h261b_engine_config_default(h261b_engine_config_t *c)
     c->fmad = 1;
     c->warps_per_cta = 0;
     c->max_ctas = 0;
-    c->use_graphs = 0;
+    c->copy_threads = 0;
 }
 
 extern "C" int64_t h261b_session_bytes(int32_t w, int32_t h)
@@ -203,11 +225,34 @@ extern "C" int64_t h261b_session_bytes(int32_t w, int32_t h)
     return (int64_t)(2 * PictureLayout::of(w, h).bytes + align_up(sizeof(h261b_denoise_dev_t), 256));
 }
 
+/* return retired session slots whose last step has completed */
+static void reclaim(h261b_engine_t *e)
+{
+    size_t k = 0;
+    for (size_t i = 0; i < e->retired.size(); i++) {
+        if (e->retired[i].last_step <= e->done_step)
+            e->pool.put(e->retired[i].bytes, e->retired[i].block);
+        else
+            e->retired[k++] = e->retired[i];
+    }
+    e->retired.resize(k);
+}
+
+static int sync_all(h261b_engine_t *e)
+{
+    for (int p = 0; p < 2; p++)
+        H261B_CUDA_TRY(cudaStreamSynchronize(e->stream[p]));
+    e->done_step = e->next_step - 1;
+    reclaim(e);
+    return H261B_OK;
+}
+
 extern "C" int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engine_t **out)
 {
     clear_error();
     if (!cfg || !out || cfg->max_sessions < 1 || cfg->max_sessions > 65536 || cfg->warps_per_cta < 0 ||
-        cfg->warps_per_cta > 8 || (cfg->me_mode != 0 && cfg->me_mode != 1)) {
+        cfg->warps_per_cta > 8 || (cfg->me_mode != 0 && cfg->me_mode != 1) || cfg->copy_threads < 0 ||
+        cfg->copy_threads > 64) {
         set_error("h261b_engine_create: bad configuration");
         return H261B_ERR_ARG;
     }
@@ -221,32 +266,35 @@ extern "C" int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engin
     h261b_engine_t *e = new h261b_engine_s();
     e->cfg = *cfg;
     e->sessions.resize((size_t)cfg->max_sessions);
+    int copiers = cfg->copy_threads;
+    if (copiers == 0)
+        copiers = std::max(1, std::min(8, (int)std::thread::hardware_concurrency() / 2));
+    e->copier.reset(new CopyPool(copiers - 1));   /* the caller is one of them */
     cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess || h261b_set_quant_table() != 0 ||
-        cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    bool ok = cudaGetDeviceProperties(&prop, cfg->device) == cudaSuccess && h261b_set_quant_table() == 0;
+    for (int p = 0; p < 2 && ok; p++) {
+        ok = cudaStreamCreateWithFlags(&e->stream[p], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&e->h2d_done[p], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&e->kernel_done[p], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&e->step_done[p], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreate(&e->k_start[p]) == cudaSuccess && cudaEventCreate(&e->k_end[p]) == cudaSuccess;
+    }
+    if (!ok) {
         set_error("h261b_engine_create: device setup failed: %s", cudaGetErrorString(cudaGetLastError()));
-        delete e;
+        h261b_engine_destroy(e);
         return H261B_ERR_CUDA;
     }
     e->sm_count = prop.multiProcessorCount;
-    for (int p = 0; p < 2; p++) {
-        cudaEventCreateWithFlags(&e->h2d_done[p], cudaEventDisableTiming);
-        cudaEventCreateWithFlags(&e->step_done[p], cudaEventDisableTiming);
-    }
-    cudaEventCreate(&e->k_start);
-    cudaEventCreate(&e->k_end);
     if (cfg->warps_per_cta > 0) {
         e->warps = cfg->warps_per_cta;
         e->ctas = cfg->max_ctas;
         e->tuned = true;
     } else {
-        /* launch shapes tried on the first steps: warps per CTA x grid cap
-         * in waves of resident CTAs (0 = one CTA per work chunk) */
-        const int wl[3] = { 2, 4, 8 };
-        for (int w : wl) {
+        /* launch shapes tried on the first steps: warps per CTA, each with a
+         * grid of one wave of resident CTAs */
+        const int wl[4] = { 2, 4, 8, 4 };
+        for (int w : wl)
             e->tune_cands.push_back({ w, 0 });
-            e->tune_cands.push_back({ w, e->sm_count * (64 / w) });
-        }
     }
     *out = e;
     return H261B_OK;
@@ -257,17 +305,21 @@ extern "C" int h261b_engine_destroy(h261b_engine_t *e)
     if (!e)
         return H261B_OK;
     cudaSetDevice(e->cfg.device);
-    cudaStreamSynchronize(e->stream);
+    for (int p = 0; p < 2; p++)
+        if (e->stream[p])
+            cudaStreamSynchronize(e->stream[p]);
     for (int p = 0; p < 2; p++) {
         e->upload[p].release();
         e->results[p].release();
         e->desc[p].release();
         cudaEventDestroy(e->h2d_done[p]);
+        cudaEventDestroy(e->kernel_done[p]);
         cudaEventDestroy(e->step_done[p]);
+        cudaEventDestroy(e->k_start[p]);
+        cudaEventDestroy(e->k_end[p]);
+        if (e->stream[p])
+            cudaStreamDestroy(e->stream[p]);
     }
-    cudaEventDestroy(e->k_start);
-    cudaEventDestroy(e->k_end);
-    cudaStreamDestroy(e->stream);
     delete e;
     return H261B_OK;
 }
@@ -306,6 +358,11 @@ extern "C" int h261b_session_open(h261b_engine_t *e, const h261b_session_config_
         return H261B_ERR_BUDGET;
     }
     cudaSetDevice(e->cfg.device);
+    reclaim(e);
+    void *blk = nullptr;
+    int rc = e->pool.get((size_t)need, &blk);
+    if (rc != H261B_OK)
+        return rc;
     Session &s = e->sessions[(size_t)slot];
     s = Session();
     s.w = c->width;
@@ -317,23 +374,24 @@ extern "C" int h261b_session_open(h261b_engine_t *e, const h261b_session_config_
     s.intra_period = c->intra_period;
     s.lay = PictureLayout::of(s.w, s.h);
     s.slot_bytes = (size_t)need;
-    void *blk = nullptr;
-    int rc = e->pool.get(s.slot_bytes, &blk);
-    if (rc != H261B_OK)
-        return rc;
     uint8_t *base = (uint8_t *)blk;
     s.rec[0] = base;
     s.rec[1] = base + s.lay.bytes;
     s.dn = (h261b_denoise_dev_t *)(base + 2 * s.lay.bytes);
     /* the first reference is black like the reference's zeroed frame
      * (h261_main.c:155-157); denoise state starts at zero
-     * (gpu_device.cu:495-508) */
+     * (gpu_device.cu:495-508).  No step in flight touches this slot (a
+     * closed slot returns to the pool only after its last step), and the
+     * clearing goes on the stream of the next step: every later step waits
+     * for that one's kernel, so none can read the slot before it is clear.
+     * The pageable source of the state copy is staged before the call
+     * returns. */
     h261b_denoise_dev_t dn0;
     memset(&dn0, 0, sizeof(dn0));
     dn0.denoise = c->denoise;
-    H261B_CUDA_TRY(cudaMemsetAsync(base, 0, 2 * s.lay.bytes, e->stream));
-    H261B_CUDA_TRY(cudaMemcpyAsync(s.dn, &dn0, sizeof(dn0), cudaMemcpyHostToDevice, e->stream));
-    H261B_CUDA_TRY(cudaStreamSynchronize(e->stream));
+    cudaStream_t st = e->stream[e->next_step & 1];
+    H261B_CUDA_TRY(cudaMemsetAsync(base, 0, 2 * s.lay.bytes, st));
+    H261B_CUDA_TRY(cudaMemcpyAsync(s.dn, &dn0, sizeof(dn0), cudaMemcpyHostToDevice, st));
     s.open = true;
     e->open_count++;
     e->session_bytes += need;
@@ -347,9 +405,10 @@ extern "C" int h261b_session_close(h261b_engine_t *e, int32_t id)
     Session *s = get_session(e, id);
     if (!s)
         return H261B_ERR_ARG;
-    /* a step may still read the session's pictures */
-    H261B_CUDA_TRY(cudaStreamSynchronize(e->stream));
-    e->pool.put(s->slot_bytes, s->rec[0]);
+    /* steps already issued may still read or write the slot: it goes back
+     * to the pool once the last of them has completed */
+    e->retired.push_back({ s->rec[0], s->slot_bytes, e->next_step - 1 });
+    reclaim(e);
     e->session_bytes -= (int64_t)s->slot_bytes;
     e->open_count--;
     *s = Session();
@@ -357,8 +416,8 @@ extern "C" int h261b_session_close(h261b_engine_t *e, int32_t id)
 }
 
 /* grow the arenas of parity p to hold a step of every open session; the
- * queued part of the upload arena is kept, results of the other parity
- * (the last step, still readable by the caller) are not touched */
+ * queued part of the upload arena is kept, arenas of the other parity (the
+ * previous step, still readable by the caller) are not touched */
 static int ensure_capacity(h261b_engine_t *e, int p)
 {
     size_t up = 0, res = 0;
@@ -372,13 +431,48 @@ static int ensure_capacity(h261b_engine_t *e, int p)
     const size_t desc = align_up((size_t)n * sizeof(h261b_session_dev_t), 256) +
                         (size_t)n * H261B_MAX_MB_PER_SESSION * sizeof(uint32_t);
     if (up > e->upload[p].cap || res > e->results[p].cap || desc > e->desc[p].cap) {
-        H261B_CUDA_TRY(cudaStreamSynchronize(e->stream));
+        H261B_CUDA_TRY(cudaStreamSynchronize(e->stream[p]));
         int rc;
-        const size_t keep = (p == e->parity && e->upload_checked) ? e->upload_used : 0;
+        const size_t keep = e->upload_checked ? e->upload_used : 0;
         if ((rc = e->upload[p].reserve(up, keep)) || (rc = e->results[p].reserve(res)) ||
             (rc = e->desc[p].reserve(desc)))
             return rc;
     }
+    return H261B_OK;
+}
+
+/* room for one picture of session s in the next step's upload arena */
+static int reserve_input(h261b_engine_t *e, Session *s, int32_t id, int32_t quant, size_t *off, const char *who)
+{
+    if (quant > 31) {
+        set_error("%s: QUANT %d out of range", who, quant);
+        return H261B_ERR_ARG;
+    }
+    if (s->queued) {
+        set_error("%s: session %d already has a queued picture", who, id);
+        return H261B_ERR_STATE;
+    }
+    const int p = (int)(e->next_step & 1);
+    int rc = ensure_capacity(e, p);
+    if (rc)
+        return rc;
+    if (!e->upload_checked) {
+        /* the copy that last read this pinned arena (two steps ago) must be
+         * complete before the host writes into it */
+        if (e->in_flight[p])
+            H261B_CUDA_TRY(cudaEventSynchronize(e->h2d_done[p]));
+        e->upload_checked = true;
+        e->upload_used = 0;
+    }
+    *off = e->upload_used;
+    if (*off + s->lay.bytes > e->upload[p].cap) {
+        set_error("%s: upload arena overflow", who);
+        return H261B_ERR_STATE;
+    }
+    e->upload_used = *off + align_up(s->lay.bytes, 256);
+    s->src_off = *off;
+    s->queued = true;
+    s->queued_quant = quant > 0 ? quant : 0;
     return H261B_OK;
 }
 
@@ -387,39 +481,126 @@ extern "C" int h261b_session_submit(h261b_engine_t *e, int32_t id, const uint8_t
 {
     clear_error();
     Session *s = get_session(e, id);
-    if (!s || !y || !cb || !cr || quant > 31) {
+    if (!s || !y || !cb || !cr) {
         if (s)
-            set_error("h261b_session_submit: bad argument");
+            set_error("h261b_session_submit: NULL plane");
         return H261B_ERR_ARG;
     }
-    if (s->queued) {
-        set_error("h261b_session_submit: session %d already has a queued picture", id);
-        return H261B_ERR_STATE;
-    }
-    int rc = ensure_capacity(e, e->parity);
+    size_t off = 0;
+    int rc = reserve_input(e, s, id, quant, &off, "h261b_session_submit");
     if (rc)
         return rc;
-    Mirror &up = e->upload[e->parity];
-    if (!e->upload_checked) {
-        /* the copy that last read this pinned arena must be complete */
-        if (e->in_flight[e->parity])
-            H261B_CUDA_TRY(cudaEventSynchronize(e->h2d_done[e->parity]));
-        e->upload_checked = true;
-        e->upload_used = 0;
-    }
-    const size_t off = e->upload_used;
-    if (off + s->lay.bytes > up.cap) {
-        set_error("h261b_session_submit: upload arena overflow");
-        return H261B_ERR_STATE;
-    }
+    uint8_t *dst = e->upload[e->next_step & 1].host + off;
     const size_t ny = (size_t)s->w * s->h, nc = ny / 4;
-    memcpy(up.host + off + s->lay.off_y, y, ny);
-    memcpy(up.host + off + s->lay.off_cb, cb, nc);
-    memcpy(up.host + off + s->lay.off_cr, cr, nc);
-    e->upload_used = off + align_up(s->lay.bytes, 256);
-    s->src_off = off;
-    s->queued = true;
-    s->queued_quant = quant > 0 ? quant : 0;
+    memcpy(dst + s->lay.off_y, y, ny);
+    memcpy(dst + s->lay.off_cb, cb, nc);
+    memcpy(dst + s->lay.off_cr, cr, nc);
+    return H261B_OK;
+}
+
+extern "C" int h261b_engine_inputs(h261b_engine_t *e, int32_t n, const int32_t *ids, const int32_t *quants,
+                                   uint8_t **staging, int64_t *offsets)
+{
+    clear_error();
+    if (!e || n < 0 || (n > 0 && (!ids || !offsets)) || !staging) {
+        set_error("h261b_engine_inputs: bad arguments");
+        return H261B_ERR_ARG;
+    }
+    for (int32_t i = 0; i < n; i++)
+        if (!get_session(e, ids[i])) {
+            set_error("h261b_engine_inputs: session %d is not open", ids[i]);
+            return H261B_ERR_ARG;
+        }
+    const size_t used0 = e->upload_used;
+    for (int32_t i = 0; i < n; i++) {
+        Session *s = get_session(e, ids[i]);
+        size_t off = 0;
+        int rc = reserve_input(e, s, ids[i], quants ? quants[i] : 0, &off, "h261b_engine_inputs");
+        if (rc) {
+            /* undo the reservations of this call */
+            for (int32_t j = 0; j < i; j++) {
+                Session *t = get_session(e, ids[j]);
+                t->queued = false;
+                t->queued_quant = 0;
+            }
+            e->upload_used = used0;
+            return rc;
+        }
+        offsets[3 * i] = (int64_t)(off + s->lay.off_y);
+        offsets[3 * i + 1] = (int64_t)(off + s->lay.off_cb);
+        offsets[3 * i + 2] = (int64_t)(off + s->lay.off_cr);
+    }
+    *staging = e->upload[e->next_step & 1].host;
+    return H261B_OK;
+}
+
+extern "C" int h261b_engine_submit_batch(h261b_engine_t *e, int32_t n, const int32_t *ids, const uint8_t *const *y,
+                                         const uint8_t *const *cb, const uint8_t *const *cr, const int32_t *quants)
+{
+    clear_error();
+    if (!e || n < 0 || (n > 0 && (!ids || !y || !cb || !cr))) {
+        set_error("h261b_engine_submit_batch: bad arguments");
+        return H261B_ERR_ARG;
+    }
+    for (int32_t i = 0; i < n; i++)
+        if (!y[i] || !cb[i] || !cr[i]) {
+            set_error("h261b_engine_submit_batch: NULL plane for picture %d", i);
+            return H261B_ERR_ARG;
+        }
+    std::vector<int64_t> offs((size_t)n * 3);
+    uint8_t *staging = nullptr;
+    int rc = h261b_engine_inputs(e, n, ids, quants, &staging, offs.data());
+    if (rc)
+        return rc;
+    std::vector<CopyJob> &jobs = e->copy_jobs;
+    jobs.clear();
+    for (int32_t i = 0; i < n; i++) {
+        const Session &s = e->sessions[(size_t)ids[i]];
+        const size_t ny = (size_t)s.w * s.h, nc = ny / 4;
+        jobs.push_back({ staging + offs[3 * i], y[i], ny });
+        jobs.push_back({ staging + offs[3 * i + 1], cb[i], nc });
+        jobs.push_back({ staging + offs[3 * i + 2], cr[i], nc });
+    }
+    e->copier->run(jobs);
+    return H261B_OK;
+}
+
+extern "C" int h261b_engine_step_records(h261b_engine_t *e, const h261b_mb_result_t **records, int64_t *count,
+                                         int64_t *step)
+{
+    clear_error();
+    if (!e || !records || !count || !step)
+        return H261B_ERR_ARG;
+    *step = e->done_step;
+    if (e->done_step < 0) {
+        *records = nullptr;
+        *count = 0;
+        return H261B_OK;
+    }
+    const int p = (int)(e->done_step & 1);
+    *records = (const h261b_mb_result_t *)e->results[p].host;
+    *count = e->step_mbs[p];
+    return H261B_OK;
+}
+
+extern "C" int h261b_session_input(h261b_engine_t *e, int32_t id, int32_t quant, uint8_t **y, uint8_t **cb,
+                                   uint8_t **cr)
+{
+    clear_error();
+    Session *s = get_session(e, id);
+    if (!s || !y || !cb || !cr) {
+        if (s)
+            set_error("h261b_session_input: NULL output pointer");
+        return H261B_ERR_ARG;
+    }
+    size_t off = 0;
+    int rc = reserve_input(e, s, id, quant, &off, "h261b_session_input");
+    if (rc)
+        return rc;
+    uint8_t *dst = e->upload[e->next_step & 1].host + off;
+    *y = dst + s->lay.off_y;
+    *cb = dst + s->lay.off_cb;
+    *cr = dst + s->lay.off_cr;
     return H261B_OK;
 }
 
@@ -465,7 +646,8 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
     if (!e)
         return H261B_ERR_ARG;
     cudaSetDevice(e->cfg.device);
-    const int p = e->parity;
+    const int64_t id = e->next_step;
+    const int p = (int)(id & 1);
     std::vector<int32_t> list;
     for (size_t i = 0; i < e->sessions.size(); i++)
         if (e->sessions[i].open && e->sessions[i].queued)
@@ -475,16 +657,25 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
     int rc = ensure_capacity(e, p);
     if (rc)
         return rc;
-    /* results and descriptors of this parity were last used two steps ago */
-    if (e->in_flight[p])
+    /* arenas of this parity were last used by step id-2 */
+    if (e->in_flight[p] && id - 2 > e->done_step) {
         H261B_CUDA_TRY(cudaEventSynchronize(e->step_done[p]));
+        e->done_step = id - 2;
+        reclaim(e);
+    }
 
     Mirror &dm = e->desc[p], &rm = e->results[p], &um = e->upload[p];
     const size_t n = list.size();
     h261b_session_dev_t *desc = (h261b_session_dev_t *)dm.host;
     const size_t work_off = align_up(n * sizeof(h261b_session_dev_t), 256);
     uint32_t *work = (uint32_t *)(dm.host + work_off);
-    size_t res_off = 0;
+    /* results arena: the MB records of all sessions back to back, then the
+     * levels of each session on a 256-byte boundary */
+    int64_t total_mb = 0;
+    for (int32_t sid : list)
+        total_mb += e->sessions[(size_t)sid].nmb;
+    size_t info_off = 0;
+    size_t res_off = align_up((size_t)total_mb * sizeof(h261b_mb_info_t), 256);
     int32_t n_work = 0;
     for (size_t k = 0; k < n; k++) {
         Session &s = e->sessions[(size_t)list[k]];
@@ -520,45 +711,54 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
         d.me_mode = e->cfg.me_mode;
         d.skip_search = intra;
         d.dn = s.dn;
-        s.info_off = res_off;
-        d.info_out = (h261b_mb_info_t *)(rm.dev + res_off);
-        res_off += align_up((size_t)s.nmb * sizeof(h261b_mb_info_t), 256);
-        s.level_off = res_off;
+        Result &r = s.res[p];
+        r.step = id;
+        r.frame = s.frame_index;
+        r.type = d.frame_type;
+        r.quant = s.quant;
+        r.info_off = info_off;
+        d.info_out = (h261b_mb_info_t *)(rm.dev + info_off);
+        info_off += (size_t)s.nmb * sizeof(h261b_mb_info_t);
+        r.level_off = res_off;
         d.level_out = (int8_t *)(rm.dev + res_off);
         res_off += align_up((size_t)s.nmb * 384, 256);
         for (int32_t m = 0; m < s.nmb; m++)
             work[n_work++] = ((uint32_t)k << 12) | (uint32_t)m;
-        s.res_frame = s.frame_index;
-        s.res_type = d.frame_type;
-        s.res_quant = s.quant;
-        s.res_parity = p;
     }
+    cudaStream_t st = e->stream[p];
     const size_t desc_bytes = work_off + (size_t)n_work * sizeof(uint32_t);
-    H261B_CUDA_TRY(cudaMemcpyAsync(dm.dev, dm.host, desc_bytes, cudaMemcpyHostToDevice, e->stream));
-    if (e->upload_used)
-        H261B_CUDA_TRY(cudaMemcpyAsync(um.dev, um.host, e->upload_used, cudaMemcpyHostToDevice, e->stream));
-    H261B_CUDA_TRY(cudaEventRecord(e->h2d_done[p], e->stream));
+    H261B_CUDA_TRY(cudaMemcpyAsync(dm.dev, dm.host, desc_bytes, cudaMemcpyHostToDevice, st));
+    if (e->upload_checked && e->upload_used)
+        H261B_CUDA_TRY(cudaMemcpyAsync(um.dev, um.host, e->upload_used, cudaMemcpyHostToDevice, st));
+    H261B_CUDA_TRY(cudaEventRecord(e->h2d_done[p], st));
+    /* the previous step's reconstructions are this step's references */
+    if (id > 0)
+        H261B_CUDA_TRY(cudaStreamWaitEvent(st, e->kernel_done[p ^ 1], 0));
 
     int warps, ctas;
     const int tuning = next_launch_shape(e, &warps, &ctas);
-    H261B_CUDA_TRY(cudaEventRecord(e->k_start, e->stream));
+    H261B_CUDA_TRY(cudaEventRecord(e->k_start[p], st));
     const int phases = H261B_PHASE_ME | H261B_PHASE_MD | H261B_PHASE_ENCDEC | (e->cfg.fmad ? 0x100 : 0);
     int lr = h261b_launch_step((const h261b_session_dev_t *)dm.dev, (const uint32_t *)(dm.dev + work_off), n_work,
-                               phases, warps, ctas, e->stream);
+                               phases, warps, ctas, st);
     if (lr != 0) {
         set_error("step launch failed: %s", cudaGetErrorString((cudaError_t)lr));
         return H261B_ERR_CUDA;
     }
-    H261B_CUDA_TRY(cudaEventRecord(e->k_end, e->stream));
-    H261B_CUDA_TRY(cudaMemcpyAsync(rm.host, rm.dev, res_off, cudaMemcpyDeviceToHost, e->stream));
-    H261B_CUDA_TRY(cudaEventRecord(e->step_done[p], e->stream));
+    H261B_CUDA_TRY(cudaEventRecord(e->k_end[p], st));
+    H261B_CUDA_TRY(cudaEventRecord(e->kernel_done[p], st));
+    H261B_CUDA_TRY(cudaMemcpyAsync(rm.host, rm.dev, res_off, cudaMemcpyDeviceToHost, st));
+    e->last_h2d = (int64_t)desc_bytes + (e->upload_checked ? (int64_t)e->upload_used : 0);
+    e->last_d2h = (int64_t)res_off;
+    H261B_CUDA_TRY(cudaEventRecord(e->step_done[p], st));
     e->in_flight[p] = true;
+    e->step_mbs[p] = total_mb;
 
     if (tuning) {
         /* time this candidate before moving on (tuning steps are synchronous) */
-        H261B_CUDA_TRY(cudaEventSynchronize(e->k_end));
+        H261B_CUDA_TRY(cudaEventSynchronize(e->k_end[p]));
         float ms = 0.f;
-        cudaEventElapsedTime(&ms, e->k_start, e->k_end);
+        cudaEventElapsedTime(&ms, e->k_start[p], e->k_end[p]);
         e->tune_ms.push_back(ms);
         e->tune_next++;
         if (e->tune_next == e->tune_cands.size()) {
@@ -572,21 +772,28 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
         }
     }
 
-    for (int32_t id : list) {
-        Session &s = e->sessions[(size_t)id];
+    for (int32_t sid : list) {
+        Session &s = e->sessions[(size_t)sid];
         s.queued = false;
         s.queued_quant = 0;
         s.dev_src[0] = s.dev_src[1] = s.dev_src[2] = nullptr;
         s.rec_cur ^= 1;
         s.frame_index++;
-        s.has_result = false;
     }
-    e->last_stepped = list;
-    e->last_parity = p;
-    e->parity ^= 1;
+    e->next_step = id + 1;
     e->upload_checked = false;
     e->upload_used = 0;
     return (int)n;
+}
+
+static int wait_step(h261b_engine_t *e, int64_t id)
+{
+    if (id < 0 || id <= e->done_step)
+        return H261B_OK;
+    H261B_CUDA_TRY(cudaEventSynchronize(e->step_done[id & 1]));
+    e->done_step = id;
+    reclaim(e);
+    return H261B_OK;
 }
 
 extern "C" int h261b_engine_sync(h261b_engine_t *e)
@@ -594,12 +801,15 @@ extern "C" int h261b_engine_sync(h261b_engine_t *e)
     clear_error();
     if (!e)
         return H261B_ERR_ARG;
-    if (e->last_parity < 0)
-        return H261B_OK;
-    H261B_CUDA_TRY(cudaEventSynchronize(e->step_done[e->last_parity]));
-    for (int32_t id : e->last_stepped)
-        e->sessions[(size_t)id].has_result = true;
-    return H261B_OK;
+    return wait_step(e, e->next_step - 1);
+}
+
+extern "C" int h261b_engine_wait_previous(h261b_engine_t *e)
+{
+    clear_error();
+    if (!e)
+        return H261B_ERR_ARG;
+    return wait_step(e, e->next_step - 2);
 }
 
 extern "C" int h261b_session_result(h261b_engine_t *e, int32_t id, h261b_frame_result_t *out)
@@ -608,17 +818,21 @@ extern "C" int h261b_session_result(h261b_engine_t *e, int32_t id, h261b_frame_r
     Session *s = get_session(e, id);
     if (!s || !out)
         return H261B_ERR_ARG;
-    if (!s->has_result) {
-        set_error("h261b_session_result: no completed step for session %d (call h261b_engine_sync)", id);
+    const Result *best = nullptr;
+    for (const Result &r : s->res)
+        if (r.step >= 0 && r.step <= e->done_step && (!best || r.step > best->step))
+            best = &r;
+    if (!best) {
+        set_error("h261b_session_result: no completed step for session %d (wait for a step first)", id);
         return H261B_ERR_STATE;
     }
-    const Mirror &rm = e->results[s->res_parity];
-    out->frame_index = s->res_frame;
-    out->frame_type = s->res_type;
-    out->quant = s->res_quant;
+    const Mirror &rm = e->results[best->step & 1];
+    out->frame_index = best->frame;
+    out->frame_type = best->type;
+    out->quant = best->quant;
     out->num_mb = s->nmb;
-    out->mbs = (const h261b_mb_result_t *)(rm.host + s->info_off);
-    out->levels = (const int8_t *)(rm.host + s->level_off);
+    out->mbs = (const h261b_mb_result_t *)(rm.host + best->info_off);
+    out->levels = (const int8_t *)(rm.host + best->level_off);
     return H261B_OK;
 }
 
@@ -629,7 +843,9 @@ extern "C" int h261b_session_recon(h261b_engine_t *e, int32_t id, uint8_t *y, ui
     if (!s || !y || !cb || !cr)
         return H261B_ERR_ARG;
     cudaSetDevice(e->cfg.device);
-    H261B_CUDA_TRY(cudaStreamSynchronize(e->stream));
+    int rc = sync_all(e);
+    if (rc)
+        return rc;
     const uint8_t *rec = s->rec[s->rec_cur];
     const size_t ny = (size_t)s->w * s->h, nc = ny / 4;
     H261B_CUDA_TRY(cudaMemcpy(y, rec + s->lay.off_y, ny, cudaMemcpyDeviceToHost));
@@ -653,10 +869,12 @@ extern "C" int h261b_result_to_abi(const h261b_frame_result_t *r, int32_t width,
         o.rgi_mv[0] = m.mvx;
         o.rgi_mv[1] = m.mvy;
         o.i_coded_block_pattern = (uint8_t)m.cbp;
+        /* compact levels are column-major per block: [b][u][v] */
         const int8_t *lv = r->levels + (size_t)i * 384;
         for (int b = 0; b < 6; b++)
-            for (int k = 0; k < 64; k++)
-                o.rgi_tcoeff[b][k] = lv[b * 64 + k];
+            for (int u = 0; u < 8; u++)
+                for (int v = 0; v < 8; v++)
+                    o.rgi_tcoeff[b][v * 8 + u] = lv[b * 64 + u * 8 + v];
         if (m.type == H261B_MB_TYPE_INTRA)
             for (int b = 0; b < 6; b++)
                 o.rgi_tcoeff[b][0] = (uint8_t)lv[b * 64];
@@ -668,10 +886,20 @@ extern "C" int h261b_result_to_abi(const h261b_frame_result_t *r, int32_t width,
 
 extern "C" int h261b_engine_last_kernel_ms(h261b_engine_t *e, float *ms)
 {
-    if (!e || !ms)
+    if (!e || !ms || e->next_step == 0)
         return H261B_ERR_ARG;
-    H261B_CUDA_TRY(cudaEventSynchronize(e->k_end));
-    H261B_CUDA_TRY(cudaEventElapsedTime(ms, e->k_start, e->k_end));
+    const int p = (int)((e->next_step - 1) & 1);
+    H261B_CUDA_TRY(cudaEventSynchronize(e->k_end[p]));
+    H261B_CUDA_TRY(cudaEventElapsedTime(ms, e->k_start[p], e->k_end[p]));
+    return H261B_OK;
+}
+
+extern "C" int h261b_engine_last_copy_bytes(h261b_engine_t *e, int64_t *h2d, int64_t *d2h)
+{
+    if (!e || !h2d || !d2h)
+        return H261B_ERR_ARG;
+    *h2d = e->last_h2d;
+    *d2h = e->last_d2h;
     return H261B_OK;
 }
 

@@ -19,14 +19,19 @@
 #define H261B_MAX_MB_PER_SESSION 4096
 
 /* per-session denoise state: the reference's h261_dct_denoise_t
- * (src/h261_types.h:122-132) split into this frame's offsets and the
- * accumulators of the frame being coded, plus the frame-end ticket */
+ * (src/h261_types.h:122-132) split into the shrink offsets of the current
+ * frame and the accumulators of the frame being coded, plus the frame-end
+ * ticket.  The offsets are kept the way the reference's kernel uses them,
+ * as UInt16 (mbgpu_kernels.cuh:513, :525-529), column-major so that a lane
+ * holding one coefficient column reads its eight offsets with one load. */
 typedef struct {
     int32_t denoise;
-    uint32_t ticket;          /* MBs of the current frame finished          */
-    int32_t count[2];         /* blocks coded this frame: [0] intra [1] inter */
-    int32_t noise[2][64];     /* sum of |coefficient| before shrinking       */
-    int32_t offset[2][64];    /* shrink offsets used by the current frame    */
+    uint32_t ticket;              /* MBs of the current frame published      */
+    int32_t count[2];             /* blocks coded this frame: [0] intra [1] inter */
+    int32_t noise[2][64];         /* sum of |coefficient| before shrinking,
+                                     raster position v * 8 + u               */
+    uint16_t offset[2][8][8];     /* [type][column u][row v]                */
+    uint8_t reserved[256];        /* keeps the state at 1040 bytes          */
 } h261b_denoise_dev_t;
 
 /* compact per-MB result of the batched path (16 bytes) */
@@ -61,7 +66,8 @@ typedef struct {
     h261_mb_mode_decision_t *md_out;
     h261_macroblock_t *abi_out;   /* reference layout, int32 levels         */
     h261b_mb_info_t *info_out;    /* compact layout                         */
-    int8_t *level_out;            /* [nmb][6][64]; intra DC stored as uint8  */
+    int8_t *level_out;            /* [nmb][6][64], per block column-major
+                                     ([u][v]); an intra DC stored as uint8   */
 } h261b_session_dev_t;
 
 /* phases a launch runs for each MB */

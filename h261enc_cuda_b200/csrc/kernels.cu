@@ -2,18 +2,21 @@
  * kernels.cu -- the sm_100a encode core: one warp per macroblock.
  *
  * A launch covers a flat list of (session, MB) work items, one frame-step
- * of any number of sessions of mixed size.  Each warp takes work items in a
- * grid-stride loop and runs, for its MB, the phases the launch asks for:
+ * of any number of sessions of mixed size.  The grid is one wave of
+ * resident CTAs; each warp owns a contiguous run of work items (consecutive
+ * MBs of mostly one session) and, for each MB, runs the phases the launch
+ * asks for while the next MB's inputs are already on their way:
  *
- *   ME      stage the 46x48 luma search window and the source MB in shared
- *           memory (16-byte loads), then
- *             - reference mode: SAD over the 11x11 coarse grid of
- *               megpu_kernels.cuh:27-166, then the 7x7 refinement of
- *               :307-446 around its winner;
- *             - full mode: every vector of [-15,15]^2;
+ *   stage   cp.async copies of the 46x48 luma search window (rows mb_y-15 ..
+ *           +30, columns mb_x-16 .. +31) and of the source MB into one of
+ *           two per-warp shared-memory buffers, issued one MB ahead.
+ *   ME      - reference mode: SAD over the 11x11 coarse grid of
+ *             megpu_kernels.cuh:27-166, then the 7x7 refinement of :307-446
+ *             around its winner; full mode: every vector of [-15,15]^2;
  *           four packed pixels per step (__vabsdiffu4 + __dp4a on funnel-
- *           shifted words).  The reference picks a winner with a 2-D tree of strict
- *           '<' comparisons in the order self, right, below, diagonal
+ *           shifted words), two candidates interleaved per lane with split
+ *           accumulators.  The reference picks a winner with a 2-D tree of
+ *           strict '<' comparisons in the order self, right, below, diagonal
  *           (:95-154); that tree returns the minimum cost and, among equal
  *           costs, the cell with the smallest Z-order index (x bits on even
  *           positions).  Each lane therefore folds (cost << 10 | zorder) into
@@ -27,30 +30,41 @@
  *           spelled out by intrinsics, denoise against the session's
  *           offsets (:506-636), quantisation (:644-724), dequantisation
  *           (:731-815), the AAN IDCT (:827-931) and reconstruction
- *           (:988-1277) into the session's output picture.  The last warp to
- *           finish a session's frame turns the frame's denoise statistics
- *           into the next frame's offsets (:478-503).
+ *           (:988-1277) into the session's output picture.
  *
- * No warp waits on another: the frame-end update is a ticket taken after a
- * warp's statistics are published, so a launch never spins.
+ * Denoise statistics are summed per warp over its run of MBs of one session
+ * and published when the session changes; the warp whose publication
+ * completes a session's frame (a ticket counting MBs) turns the statistics
+ * into the next frame's offsets (:478-503).  No warp waits on another.
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <mutex>
 
 #include "h261b_device.h"
 
 namespace {
 
-constexpr int WIN_ROWS = 46;        /* rows mb_y-15 .. mb_y+30              */
-constexpr int WIN_PITCH_W = 13;     /* 48 columns in 13 words (odd pitch)    */
+constexpr int WIN_ROWS = 46;        /* rows mb_y-15 .. mb_y+30               */
+constexpr int WIN_WORDS = 12;       /* columns mb_x-16 .. mb_x+31            */
+constexpr int WIN_PITCH_W = 13;     /* odd word pitch against bank conflicts */
 constexpr uint32_t FULL = 0xffffffffu;
 
-struct __align__(16) WarpSmem {
-    uint32_t win[WIN_ROWS * WIN_PITCH_W]; /* reference luma window          */
+/* one MB's staged inputs */
+struct __align__(16) StageBuf {
+    uint32_t win[WIN_ROWS * WIN_PITCH_W]; /* reference luma window           */
     uint32_t pad0[2];
-    uint32_t cur[64];                     /* source luma MB, 16 B per row   */
+    uint32_t cur[64];                     /* source luma MB, 16 B per row    */
     uint32_t curc[2][16];                 /* source Cb, Cr 8x8               */
-    float t[4][64];                       /* transpose buffer               */
+};
+
+struct __align__(16) WarpSmem {
+    StageBuf buf[2];                      /* this MB, next MB                */
+    float t[4][72];                       /* transpose buffer: row stride 9,
+                                             block stride 72 words, so both
+                                             row and column accesses of the
+                                             four blocks are conflict-free   */
 };
 
 __constant__ int8_t c_stage1[11] = { -14, -11, -8, -5, -2, 0, 2, 5, 8, 11, 14 };
@@ -81,14 +95,55 @@ __device__ __forceinline__ uint32_t compact8(uint32_t v)
 
 __device__ __forceinline__ uint32_t zorder(uint32_t x, uint32_t y) { return spread8(x) | (spread8(y) << 1); }
 
-__device__ __forceinline__ uint8_t win_byte(const WarpSmem &s, int row, int col)
+/* eight window bytes of row `row` from byte column `col` (any alignment):
+ * three word loads, two funnel shifts; col <= 43 keeps the loads inside
+ * the row's 13 words (bytes past column 47 are never used) */
+__device__ __forceinline__ uint2 win8(const StageBuf &s, int row, int col)
 {
-    return reinterpret_cast<const uint8_t *>(s.win)[row * (WIN_PITCH_W * 4) + col];
+    const uint32_t *p = s.win + row * WIN_PITCH_W + (col >> 2);
+    const uint32_t sh = (uint32_t)(col & 3) * 8u;
+    const uint32_t a = p[0], b = p[1], c = p[2];
+    return make_uint2(__funnelshift_r(a, b, sh), __funnelshift_r(b, c, sh));
 }
 
-__device__ __forceinline__ uint8_t cur_byte(const WarpSmem &s, int row, int col)
+/* eight bytes from global memory at any alignment; reads only the words
+ * that hold one of those bytes */
+__device__ __forceinline__ uint2 glob8(const uint8_t *ptr)
 {
-    return reinterpret_cast<const uint8_t *>(s.cur)[row * 16 + col];
+    const uint32_t *p = reinterpret_cast<const uint32_t *>((uintptr_t)ptr & ~(uintptr_t)3);
+    const uint32_t sh = (uint32_t)((uintptr_t)ptr & 3) * 8u;
+    const uint32_t a = p[0], b = p[1], c = sh ? p[2] : 0u;
+    return make_uint2(__funnelshift_r(a, b, sh), __funnelshift_r(b, c, sh));
+}
+
+__device__ __forceinline__ int byte8(uint2 v, int i)
+{
+    return (int)(((i < 4 ? v.x : v.y) >> (8 * (i & 3))) & 0xFFu);
+}
+
+/* asynchronous global -> shared copies; a source outside the picture is
+ * not read (src-size 0) and its bytes are zero-filled */
+__device__ __forceinline__ void cp_async4(void *dst, const void *src, bool valid)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 4 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 /* sum of |a_i - b_i| over the four bytes, added to acc: per-byte absolute
@@ -99,24 +154,34 @@ __device__ __forceinline__ uint32_t sad4(uint32_t a, uint32_t b, uint32_t acc)
     return __dp4a(__vabsdiffu4(a, b), 0x01010101u, acc);
 }
 
-/* SAD of the source MB against the window block at vector (vx, vy) */
-__device__ __forceinline__ uint32_t sad16x16(const WarpSmem &s, int vx, int vy)
+/* SADs of the source MB against the window blocks at two vectors, computed
+ * together: four accumulators keep the dependency chains short */
+__device__ __forceinline__ void sad16x16_pair(const StageBuf &s, int vx0, int vy0, int vx1, int vy1, uint32_t &s0,
+                                              uint32_t &s1)
 {
-    const int bo = 16 + vx;
-    const uint32_t *p = s.win + (15 + vy) * WIN_PITCH_W + (bo >> 2);
-    const uint32_t sh = (uint32_t)(bo & 3) * 8u;
-    uint32_t acc = 0;
+    const int b0 = 16 + vx0, b1 = 16 + vx1;
+    const uint32_t *p0 = s.win + (15 + vy0) * WIN_PITCH_W + (b0 >> 2);
+    const uint32_t *p1 = s.win + (15 + vy1) * WIN_PITCH_W + (b1 >> 2);
+    const uint32_t sh0 = (uint32_t)(b0 & 3) * 8u, sh1 = (uint32_t)(b1 & 3) * 8u;
+    uint32_t a0 = 0, a1 = 0, c0 = 0, c1 = 0;
 #pragma unroll 4
     for (int r = 0; r < 16; r++) {
-        const uint32_t a0 = p[0], a1 = p[1], a2 = p[2], a3 = p[3], a4 = p[4];
         const uint4 c = *reinterpret_cast<const uint4 *>(s.cur + 4 * r);
-        acc = sad4(c.x, __funnelshift_r(a0, a1, sh), acc);
-        acc = sad4(c.y, __funnelshift_r(a1, a2, sh), acc);
-        acc = sad4(c.z, __funnelshift_r(a2, a3, sh), acc);
-        acc = sad4(c.w, __funnelshift_r(a3, a4, sh), acc);
-        p += WIN_PITCH_W;
+        const uint32_t x0 = p0[0], x1 = p0[1], x2 = p0[2], x3 = p0[3], x4 = p0[4];
+        const uint32_t y0 = p1[0], y1 = p1[1], y2 = p1[2], y3 = p1[3], y4 = p1[4];
+        a0 = sad4(c.x, __funnelshift_r(x0, x1, sh0), a0);
+        c0 = sad4(c.x, __funnelshift_r(y0, y1, sh1), c0);
+        a1 = sad4(c.y, __funnelshift_r(x1, x2, sh0), a1);
+        c1 = sad4(c.y, __funnelshift_r(y1, y2, sh1), c1);
+        a0 = sad4(c.z, __funnelshift_r(x2, x3, sh0), a0);
+        c0 = sad4(c.z, __funnelshift_r(y2, y3, sh1), c0);
+        a1 = sad4(c.w, __funnelshift_r(x3, x4, sh0), a1);
+        c1 = sad4(c.w, __funnelshift_r(y3, y4, sh1), c1);
+        p0 += WIN_PITCH_W;
+        p1 += WIN_PITCH_W;
     }
-    return acc;
+    s0 = a0 + a1;
+    s1 = c0 + c1;
 }
 
 /* 4x4 Hadamard SATD, megpu_kernels.cuh:467-500 */
@@ -247,60 +312,52 @@ struct MbDecision {
     int32_t type, flags, mvx, mvy, cost;
 };
 
-__device__ __forceinline__ void load_sources(WarpSmem &s, const h261b_session_dev_t &S, int mbx, int mby,
-                                             int lane, bool need_window)
+/* start the asynchronous copies of one MB's inputs into b */
+__device__ __forceinline__ void stage_mb(StageBuf &b, const h261b_session_dev_t &S, int mbx, int mby, int lane)
 {
     const int W = S.mbw * 16, H = S.mbh * 16;
     const int x0 = mbx * 16, y0 = mby * 16;
-    if (need_window) {
-        /* 46 rows x 3 chunks of 16 pixels; chunks outside the frame are
-         * zero (no search vector ever reaches them) */
-        for (int t = lane; t < WIN_ROWS * 3; t += 32) {
-            const int r = t / 3, c = t - r * 3;
-            const int y = y0 - 15 + r, x = x0 - 16 + 16 * c;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (y >= 0 && y < H && x >= 0 && x < W)
-                v = *reinterpret_cast<const uint4 *>(S.ref_y + (size_t)y * S.pitch_y + x);
-            uint32_t *d = s.win + r * WIN_PITCH_W + 4 * c;
-            d[0] = v.x;
-            d[1] = v.y;
-            d[2] = v.z;
-            d[3] = v.w;
-        }
+    for (int t = lane; t < WIN_ROWS * WIN_WORDS; t += 32) {
+        const int r = t / WIN_WORDS, w = t - r * WIN_WORDS;
+        const int y = y0 - 15 + r, x = x0 - 16 + 4 * w;
+        const bool ok = y >= 0 && y < H && x >= 0 && x < W;
+        cp_async4(&b.win[r * WIN_PITCH_W + w], ok ? S.ref_y + (size_t)y * S.pitch_y + x : S.ref_y, ok);
     }
     if (lane < 16) {
-        const uint4 v = *reinterpret_cast<const uint4 *>(S.cur_y + (size_t)(y0 + lane) * S.pitch_y + x0);
-        *reinterpret_cast<uint4 *>(s.cur + 4 * lane) = v;
+        cp_async16(&b.cur[4 * lane], S.cur_y + (size_t)(y0 + lane) * S.pitch_y + x0);
     } else {
         const int k = lane - 16, pl = k >> 3, r = k & 7;
         const uint8_t *src = pl ? S.cur_cr : S.cur_cb;
-        const uint2 v = *reinterpret_cast<const uint2 *>(src + (size_t)(mby * 8 + r) * S.pitch_c + mbx * 8);
-        s.curc[pl][2 * r] = v.x;
-        s.curc[pl][2 * r + 1] = v.y;
+        cp_async8(&b.curc[pl][2 * r], src + (size_t)(mby * 8 + r) * S.pitch_c + mbx * 8);
     }
-    __syncwarp();
 }
 
 /* motion search + SATD costs; results are warp-uniform */
-__device__ __forceinline__ void motion_estimate(const WarpSmem &s, const h261b_session_dev_t &S, int mbx,
-                                                int mby, int lane, me_gpu_mb_t &res, int8_t &s1x,
-                                                int8_t &s1y)
+__device__ __forceinline__ void motion_estimate(const StageBuf &s, const h261b_session_dev_t &S, int mbx, int mby,
+                                                int lane, me_gpu_mb_t &res, int8_t &s1x, int8_t &s1y)
 {
     const int bx = mbx * 16, by = mby * 16;
     /* per-MB limits, gpu_device.cu:226-265 */
     const int lminx = max(-15, -bx), lmaxx = min(15, (S.mbw - 1) * 16 - bx);
     const int lminy = max(-15, -by), lmaxy = min(15, (S.mbh - 1) * 16 - by);
     int vx, vy;
+    /* every lane computes two SADs per iteration; a vector outside the
+     * limits is replaced by (0, 0) so no address leaves the window, and its
+     * cost discarded (65535, as the reference marks skipped candidates) */
     if (S.me_mode == 1) {
         uint32_t best = FULL;
-        for (int c = lane; c < 31 * 31; c += 32) {
-            const int tx = c % 31, ty = c / 31, x = tx - 15, y = ty - 15;
-            const bool ok = x >= lminx && x <= lmaxx && y >= lminy && y <= lmaxy;
-            /* every lane computes a SAD; a vector outside the limits is replaced by
-             * (0, 0) so no address leaves the window, and its cost discarded */
-            const uint32_t sad = sad16x16(s, ok ? x : 0, ok ? y : 0);
-            const uint32_t cost = ok ? sad : 65535u;
-            best = min(best, (cost << 10) | zorder(tx, ty));
+        for (int c = lane; c < 31 * 31; c += 64) {
+            const int c1 = c + 32;
+            const bool has1 = c1 < 31 * 31;
+            const int ty0 = c / 31, tx0 = c - ty0 * 31, ty1 = (has1 ? c1 : c) / 31, tx1 = (has1 ? c1 : c) - ty1 * 31;
+            const int x0 = tx0 - 15, y0 = ty0 - 15, x1 = tx1 - 15, y1 = ty1 - 15;
+            const bool o0 = x0 >= lminx && x0 <= lmaxx && y0 >= lminy && y0 <= lmaxy;
+            const bool o1 = has1 && x1 >= lminx && x1 <= lmaxx && y1 >= lminy && y1 <= lmaxy;
+            uint32_t s0, s1;
+            sad16x16_pair(s, o0 ? x0 : 0, o0 ? y0 : 0, o1 ? x1 : 0, o1 ? y1 : 0, s0, s1);
+            best = min(best, ((o0 ? s0 : 65535u) << 10) | zorder(tx0, ty0));
+            if (has1)
+                best = min(best, ((o1 ? s1 : 65535u) << 10) | zorder(tx1, ty1));
         }
         best = __reduce_min_sync(FULL, best) & 1023u; /* Z-order index only */
         vx = (int)compact8(best) - 15;
@@ -308,60 +365,75 @@ __device__ __forceinline__ void motion_estimate(const WarpSmem &s, const h261b_s
         s1x = s1y = 0;
     } else {
         uint32_t best = FULL;
-        for (int c = lane; c < 121; c += 32) {
-            const int ty = c / 11, tx = c - ty * 11;
-            const int x = c_stage1[tx], y = c_stage1[ty];
-            const bool ok = x >= lminx && x <= lmaxx && y >= lminy && y <= lmaxy;
-            /* every lane computes a SAD; a vector outside the limits is replaced by
-             * (0, 0) so no address leaves the window, and its cost discarded */
-            const uint32_t sad = sad16x16(s, ok ? x : 0, ok ? y : 0);
-            const uint32_t cost = ok ? sad : 65535u;
-            best = min(best, (cost << 10) | zorder(tx, ty));
+        for (int c = lane; c < 121; c += 64) {
+            const int c1 = c + 32;
+            const bool has1 = c1 < 121;
+            const int ty0 = c / 11, tx0 = c - ty0 * 11, ty1 = (has1 ? c1 : c) / 11, tx1 = (has1 ? c1 : c) - ty1 * 11;
+            const int x0 = c_stage1[tx0], y0 = c_stage1[ty0], x1 = c_stage1[tx1], y1 = c_stage1[ty1];
+            const bool o0 = x0 >= lminx && x0 <= lmaxx && y0 >= lminy && y0 <= lmaxy;
+            const bool o1 = has1 && x1 >= lminx && x1 <= lmaxx && y1 >= lminy && y1 <= lmaxy;
+            uint32_t s0, s1;
+            sad16x16_pair(s, o0 ? x0 : 0, o0 ? y0 : 0, o1 ? x1 : 0, o1 ? y1 : 0, s0, s1);
+            best = min(best, ((o0 ? s0 : 65535u) << 10) | zorder(tx0, ty0));
+            if (has1)
+                best = min(best, ((o1 ? s1 : 65535u) << 10) | zorder(tx1, ty1));
         }
         best = __reduce_min_sync(FULL, best) & 1023u; /* Z-order index only */
         const int v1x = c_stage1[compact8(best)], v1y = c_stage1[compact8(best >> 1)];
         s1x = (int8_t)v1x;
         s1y = (int8_t)v1y;
         best = FULL;
-        for (int c = lane; c < 49; c += 32) {
-            const int ty = c / 7, tx = c - ty * 7;
-            const int x = v1x + tx - 3, y = v1y + ty - 3;
-            const bool ok = x >= lminx && x <= lmaxx && y >= lminy && y <= lmaxy;
-            /* every lane computes a SAD; a vector outside the limits is replaced by
-             * (0, 0) so no address leaves the window, and its cost discarded */
-            const uint32_t sad = sad16x16(s, ok ? x : 0, ok ? y : 0);
-            const uint32_t cost = ok ? sad : 65535u;
-            best = min(best, (cost << 10) | zorder(tx, ty));
+        {
+            const int c = lane, c1 = lane + 32;
+            const bool has1 = c1 < 49;
+            const int ty0 = c / 7, tx0 = c - ty0 * 7, ty1 = (has1 ? c1 : c) / 7, tx1 = (has1 ? c1 : c) - ty1 * 7;
+            const int x0 = v1x + tx0 - 3, y0 = v1y + ty0 - 3, x1 = v1x + tx1 - 3, y1 = v1y + ty1 - 3;
+            const bool o0 = x0 >= lminx && x0 <= lmaxx && y0 >= lminy && y0 <= lmaxy;
+            const bool o1 = has1 && x1 >= lminx && x1 <= lmaxx && y1 >= lminy && y1 <= lmaxy;
+            uint32_t s0, s1;
+            sad16x16_pair(s, o0 ? x0 : 0, o0 ? y0 : 0, o1 ? x1 : 0, o1 ? y1 : 0, s0, s1);
+            best = min(best, ((o0 ? s0 : 65535u) << 10) | zorder(tx0, ty0));
+            if (has1)
+                best = min(best, ((o1 ? s1 : 65535u) << 10) | zorder(tx1, ty1));
         }
-        best = __reduce_min_sync(FULL, best) & 1023u; /* Z-order index only */
+        best = __reduce_min_sync(FULL, best) & 1023u;
         vx = v1x + (int)compact8(best) - 3;
         vy = v1y + (int)compact8(best >> 1) - 3;
     }
 
     /* costs at the final vector: lanes 0-15 inter, 16-31 filtered inter,
-     * one 4x4 sub-block each; then intra on lanes 0-15 */
+     * one 4x4 sub-block each; then intra on lanes 0-15.  Each lane reads
+     * six window rows around its sub-block (clamped to the window: a
+     * clamped row is one the sub-block never needs) from one column left of
+     * it, so pixel (iy, ix) is byte ix + 1 of row iy + 1 */
     const int sb = lane & 15, sx = sb & 3, sy = sb >> 2;
     const bool filt = lane >= 16;
+    const int wr0 = 15 + vy + sy * 4, wc0 = 16 + vx + sx * 4;
+    uint2 rr[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++)
+        rr[k] = win8(s, min(max(wr0 - 1 + k, 0), WIN_ROWS - 1), wc0 - 1);
     int32_t d[16], di[16];
 #pragma unroll
-    for (int iy = 0; iy < 4; iy++)
+    for (int iy = 0; iy < 4; iy++) {
+        const uint32_t cw = s.cur[(sy * 4 + iy) * 4 + sx];
 #pragma unroll
         for (int ix = 0; ix < 4; ix++) {
-            const int cx = sx * 4 + ix, cy = sy * 4 + iy;
-            const int c = cur_byte(s, cy, cx);
-            const int wr = 15 + vy + cy, wc = 16 + vx + cx;
+            const int c = (int)((cw >> (8 * ix)) & 0xFFu);
             const int lx = (sx & 1) * 4 + ix, ly = (sy & 1) * 4 + iy;
+            const int R = iy + 1, C = ix + 1;
             int p;
             if (filt && lx >= 1 && lx <= 6 && ly >= 1 && ly <= 6) {
-                p = (win_byte(s, wr - 1, wc - 1) + 2 * win_byte(s, wr - 1, wc) + win_byte(s, wr - 1, wc + 1) +
-                     2 * win_byte(s, wr, wc - 1) + 4 * win_byte(s, wr, wc) + 2 * win_byte(s, wr, wc + 1) +
-                     win_byte(s, wr + 1, wc - 1) + 2 * win_byte(s, wr + 1, wc) + win_byte(s, wr + 1, wc + 1) + 8) >> 4;
+                p = (byte8(rr[R - 1], C - 1) + 2 * byte8(rr[R - 1], C) + byte8(rr[R - 1], C + 1) +
+                     2 * byte8(rr[R], C - 1) + 4 * byte8(rr[R], C) + 2 * byte8(rr[R], C + 1) +
+                     byte8(rr[R + 1], C - 1) + 2 * byte8(rr[R + 1], C) + byte8(rr[R + 1], C + 1) + 8) >> 4;
             } else {
-                p = win_byte(s, wr, wc);
+                p = byte8(rr[R], C);
             }
             d[iy * 4 + ix] = c - p;
             di[iy * 4 + ix] = c;
         }
+    }
     const int32_t satd = satd4x4(d), satd_i = satd4x4(di);
     res.i_16x16_cost = (int32_t)__reduce_add_sync(FULL, filt ? 0u : (uint32_t)satd);
     res.i_16x16_filter_cost = (int32_t)__reduce_add_sync(FULL, filt ? (uint32_t)satd : 0u);
@@ -398,33 +470,24 @@ __device__ __forceinline__ MbDecision mode_decide(const me_gpu_mb_t &g, int fram
     return m;
 }
 
-/* reference pixel (row, col) of the 8x8 prediction block of block b */
-struct BlockRef {
-    const WarpSmem *s;
-    const uint8_t *g; /* chroma: top-left of the block in the ref plane */
-    int pitch;
-    int wr, wc;       /* luma: top-left of the block in the window      */
-    bool luma;
-    __device__ __forceinline__ int at(int r, int c) const
-    {
-        return luma ? win_byte(*s, wr + r, wc + c) : g[r * pitch + c];
-    }
-    /* horizontal [1 2 1] with x4 edge columns, mbgpu_kernels.cuh:88-103 */
-    __device__ __forceinline__ int h(int r, int c) const
-    {
-        if (c == 0)
-            return at(r, 0) * 4;
-        if (c == 7)
-            return at(r, 7) * 4;
-        return at(r, c - 1) + at(r, c) * 2 + at(r, c + 1);
-    }
-};
+/* H.261 loop-filter tap pair, horizontal [1 2 1] with x4 edge columns
+ * (mbgpu_kernels.cuh:88-103) on one 8-pixel row */
+__device__ __forceinline__ int hfilt(uint2 v, int c)
+{
+    if (c == 0)
+        return byte8(v, 0) * 4;
+    if (c == 7)
+        return byte8(v, 7) * 4;
+    return byte8(v, c - 1) + byte8(v, c) * 2 + byte8(v, c + 1);
+}
 
-/* one pass over up to four blocks of the MB: lane = slot * 8 + row */
+/* one pass over up to four blocks of the MB: lane = slot * 8 + row (then
+ * column).  Adds the block-summed |coefficient| of column (lane & 7) to
+ * colsum[v] and returns this pass's CBP bits. */
 template <int FMAD>
-__device__ __forceinline__ void encdec_pass(WarpSmem &s, const h261b_session_dev_t &S, int mb, int mbx,
-                                            int mby, const MbDecision &m, int quant, bool luma_pass, int lane,
-                                            int32_t stat[8], uint32_t &cbp)
+__device__ __forceinline__ uint32_t encdec_pass(float (*tb)[72], const StageBuf &s, const h261b_session_dev_t &S,
+                                                int mb, int mbx, int mby, const MbDecision &m, int quant,
+                                                bool luma_pass, int lane, int32_t colsum[8])
 {
     const bool active = luma_pass || lane < 16;
     const int slot = lane >> 3, r = lane & 7;
@@ -433,50 +496,52 @@ __device__ __forceinline__ void encdec_pass(WarpSmem &s, const h261b_session_dev
     const bool filter = (m.flags & H261B_MB_FILTER) != 0;
     const int t = intra ? 0 : 1;
 
-    /* ---- prediction and residual of row r (mbgpu_kernels.cuh:59-166) */
-    BlockRef ref;
-    ref.s = &s;
-    int bx8 = 0, by8 = 0;
-    if (luma_pass) {
-        bx8 = (b & 1) * 8;
-        by8 = (b >> 1) * 8;
-        ref.luma = true;
-        ref.wr = 15 + m.mvy + by8;
-        ref.wc = 16 + m.mvx + bx8;
-        ref.g = nullptr;
-        ref.pitch = 0;
-    } else {
-        const int cmx = m.mvx / 2, cmy = m.mvy / 2; /* truncation toward zero */
-        const uint8_t *pl = (b == 4) ? S.ref_cb : S.ref_cr;
-        ref.luma = false;
-        ref.wr = ref.wc = 0;
-        ref.pitch = S.pitch_c;
-        ref.g = pl + (size_t)(mby * 8 + cmy) * S.pitch_c + (mbx * 8 + cmx);
-    }
+    /* ---- prediction and residual of row r (mbgpu_kernels.cuh:59-166):
+     * the source row and up to three reference rows as 8-byte vectors */
+    const int bx8 = luma_pass ? (b & 1) * 8 : 0, by8 = luma_pass ? (b >> 1) * 8 : 0;
     int32_t pred[8], res[8];
 #pragma unroll
     for (int i = 0; i < 8; i++)
         pred[i] = 0;
     if (active) {
+        const uint2 cw = luma_pass ? *reinterpret_cast<const uint2 *>(&s.cur[(by8 + r) * 4 + (bx8 >> 2)])
+                                   : *reinterpret_cast<const uint2 *>(&s.curc[b - 4][2 * r]);
+        if (intra) {
 #pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const int c = luma_pass ? cur_byte(s, by8 + r, bx8 + i)
-                                    : reinterpret_cast<const uint8_t *>(s.curc[b - 4])[r * 8 + i];
-            if (intra) {
-                res[i] = c;
-                continue;
-            }
-            int p;
-            if (filter) {
-                if (r == 0 || r == 7)
-                    p = (ref.h(r, i) + 2) >> 2;
-                else
-                    p = (ref.h(r - 1, i) + ref.h(r, i) * 2 + ref.h(r + 1, i) + 8) >> 4;
+            for (int i = 0; i < 8; i++)
+                res[i] = byte8(cw, i);
+        } else {
+            /* rows r-1, r, r+1 of the prediction block, clamped inside it
+             * (the edge rows of the loop filter use row r only) */
+            const int ra_i = max(r - 1, 0), rc_i = min(r + 1, 7);
+            uint2 ra, rb, rc;
+            if (luma_pass) {
+                const int wr = 15 + m.mvy + by8, wc = 16 + m.mvx + bx8;
+                rb = win8(s, wr + r, wc);
+                ra = filter ? win8(s, wr + ra_i, wc) : rb;
+                rc = filter ? win8(s, wr + rc_i, wc) : rb;
             } else {
-                p = ref.at(r, i);
+                const int cmx = m.mvx / 2, cmy = m.mvy / 2; /* truncation toward zero */
+                const uint8_t *g = ((b == 4) ? S.ref_cb : S.ref_cr) + (size_t)(mby * 8 + cmy) * S.pitch_c +
+                                   (mbx * 8 + cmx);
+                rb = glob8(g + (size_t)r * S.pitch_c);
+                ra = filter ? glob8(g + (size_t)ra_i * S.pitch_c) : rb;
+                rc = filter ? glob8(g + (size_t)rc_i * S.pitch_c) : rb;
             }
-            pred[i] = p;
-            res[i] = c - p;
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                int p;
+                if (filter) {
+                    if (r == 0 || r == 7)
+                        p = (hfilt(rb, i) + 2) >> 2;
+                    else
+                        p = (hfilt(ra, i) + hfilt(rb, i) * 2 + hfilt(rc, i) + 8) >> 4;
+                } else {
+                    p = byte8(rb, i);
+                }
+                pred[i] = p;
+                res[i] = byte8(cw, i) - p;
+            }
         }
         /* ---- FDCT pass 1 on row r */
         float o[8];
@@ -485,35 +550,39 @@ __device__ __forceinline__ void encdec_pass(WarpSmem &s, const h261b_session_dev
                              (float)(res[1] - res[6]), (float)(res[0] - res[7]), o);
 #pragma unroll
         for (int k = 0; k < 8; k++)
-            s.t[slot][r * 8 + k] = o[k];
+            tb[slot][r * 9 + k] = o[k];
     }
     __syncwarp();
 
     /* ---- FDCT pass 2 on column c = r: coefficients (v, c), v = 0..7 */
     const int c = r;
-    int32_t lev[8];
+    int32_t lev[8], nz[8];
     int32_t acc = 0;
-    int32_t nz[8];
 #pragma unroll
     for (int v = 0; v < 8; v++) {
         lev[v] = 0;
         nz[v] = 0;
     }
     if (active) {
-        const float *p = s.t[slot] + c;
-        float o[8];
-        fdct_butterfly<FMAD>(p[0] + p[56], p[8] + p[48], p[16] + p[40], p[24] + p[32], p[24] - p[32],
-                             p[16] - p[40], p[8] - p[48], p[0] - p[56], o);
+        float q[8], o[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            q[k] = tb[slot][k * 9 + c];
+        fdct_butterfly<FMAD>(q[0] + q[7], q[1] + q[6], q[2] + q[5], q[3] + q[4], q[3] - q[4], q[2] - q[5],
+                             q[1] - q[6], q[0] - q[7], o);
         const float cs = dmulf(c_fwd_post[c], 0.125);
         const float inv = c_inv_quant[quant];
+        /* this column's eight offsets, UInt16, one 16-byte load */
+        const uint4 ow = *reinterpret_cast<const uint4 *>(&S.dn->offset[t][c][0]);
+        const uint32_t offw[4] = { ow.x, ow.y, ow.z, ow.w };
 #pragma unroll
         for (int v = 0; v < 8; v++) {
             int32_t lv = fdct_round(cs, c_fwd_post[v], o[v]);
-            /* denoise (mbgpu_kernels.cuh:586-604): offsets as UInt16 */
+            /* denoise (mbgpu_kernels.cuh:586-604) */
             const int32_t sign = lv >> 31;
             lv = (lv ^ sign) - sign;
             nz[v] = lv;
-            const int32_t off = (int32_t)(uint16_t)S.dn->offset[t][v * 8 + c];
+            const int32_t off = (int32_t)((offw[v >> 1] >> (16 * (v & 1))) & 0xFFFFu);
             lv = max(lv - off, 0);
             lv = (lv ^ sign) - sign;
             /* quant (mbgpu_kernels.cuh:689-716) */
@@ -538,7 +607,7 @@ __device__ __forceinline__ void encdec_pass(WarpSmem &s, const h261b_session_dev
     acc += __shfl_xor_sync(FULL, acc, 2);
     acc += __shfl_xor_sync(FULL, acc, 4);
     const bool coded = active && acc > 2;
-    cbp |= __reduce_or_sync(FULL, coded ? (uint32_t)H261B_CBP_BIT(b) : 0u);
+    const uint32_t cbp = __reduce_or_sync(FULL, coded ? (uint32_t)H261B_CBP_BIT(b) : 0u);
 
     /* denoise statistics: sum the same coefficient position over blocks */
 #pragma unroll
@@ -546,7 +615,7 @@ __device__ __forceinline__ void encdec_pass(WarpSmem &s, const h261b_session_dev
         int32_t x = nz[v];
         x += __shfl_xor_sync(FULL, x, 8);
         x += __shfl_xor_sync(FULL, x, 16);
-        stat[v] += x;
+        colsum[v] += x;
     }
 
     /* ---- levels out */
@@ -558,10 +627,14 @@ __device__ __forceinline__ void encdec_pass(WarpSmem &s, const h261b_session_dev
                 tc[v * 8 + c] = lev[v];
         }
         if (S.level_out) {
-            int8_t *lo = S.level_out + (size_t)mb * 384 + b * 64;
+            /* column-major: this lane's eight levels are contiguous */
+            uint32_t lo = 0, hi = 0;
 #pragma unroll
-            for (int v = 0; v < 8; v++)
-                lo[v * 8 + c] = (int8_t)lev[v];
+            for (int v = 0; v < 4; v++) {
+                lo |= ((uint32_t)lev[v] & 0xFFu) << (8 * v);
+                hi |= ((uint32_t)lev[v + 4] & 0xFFu) << (8 * v);
+            }
+            *reinterpret_cast<uint2 *>(S.level_out + (size_t)mb * 384 + b * 64 + c * 8) = make_uint2(lo, hi);
         }
     }
 
@@ -587,31 +660,31 @@ __device__ __forceinline__ void encdec_pass(WarpSmem &s, const h261b_session_dev
         }
         if (coded) {
             /* prescale: t = (coef * pre[col]) * (pre[row] * 0.125) */
-            float P[8], cs[8], t[8], o[8];
+            float P[8], cs[8], tt[8], o[8];
 #pragma unroll
             for (int k = 0; k < 8; k++) {
                 cs[k] = dmulf(c_inv_pre[k], 0.125);
                 P[k] = __fmul_rn(col[k], c_inv_pre[c]);
-                t[k] = __fmul_rn(P[k], cs[k]);
+                tt[k] = __fmul_rn(P[k], cs[k]);
             }
-            idct_rest<FMAD>(first_sub<FMAD>(P[2], cs[2], t[2], t[6]), first_add<FMAD>(P[2], cs[2], t[2], t[6]),
-                            first_add<FMAD>(P[0], cs[0], t[0], t[4]), first_sub<FMAD>(P[0], cs[0], t[0], t[4]),
-                            first_add<FMAD>(P[1], cs[1], t[1], t[7]), first_sub<FMAD>(P[1], cs[1], t[1], t[7]),
-                            first_add<FMAD>(P[5], cs[5], t[5], t[3]), first_sub<FMAD>(P[5], cs[5], t[5], t[3]), o);
+            idct_rest<FMAD>(first_sub<FMAD>(P[2], cs[2], tt[2], tt[6]), first_add<FMAD>(P[2], cs[2], tt[2], tt[6]),
+                            first_add<FMAD>(P[0], cs[0], tt[0], tt[4]), first_sub<FMAD>(P[0], cs[0], tt[0], tt[4]),
+                            first_add<FMAD>(P[1], cs[1], tt[1], tt[7]), first_sub<FMAD>(P[1], cs[1], tt[1], tt[7]),
+                            first_add<FMAD>(P[5], cs[5], tt[5], tt[3]), first_sub<FMAD>(P[5], cs[5], tt[5], tt[3]), o);
 #pragma unroll
             for (int k = 0; k < 8; k++)
-                s.t[slot][k * 8 + c] = o[k];
+                tb[slot][k * 9 + c] = o[k];
         } else {
 #pragma unroll
             for (int k = 0; k < 8; k++)
-                s.t[slot][k * 8 + c] = col[k];
+                tb[slot][k * 9 + c] = col[k];
         }
     }
     __syncwarp();
 
     /* ---- IDCT pass 2 on row r and reconstruction (mbgpu_kernels.cuh:988-1096) */
     if (active) {
-        const float *p = s.t[slot] + r * 8;
+        const float *p = tb[slot] + r * 9;
         int32_t out[8];
         if (coded) {
             float o[8];
@@ -642,6 +715,7 @@ __device__ __forceinline__ void encdec_pass(WarpSmem &s, const h261b_session_dev
         *reinterpret_cast<uint2 *>(dst) = make_uint2(lo, hi);
     }
     __syncwarp();
+    return cbp;
 }
 
 /* frame-end denoise update by the session's last warp (mbgpu_kernels.cuh:478-503) */
@@ -657,39 +731,99 @@ __device__ __forceinline__ void denoise_frame_end(h261b_denoise_dev_t *dn, int l
     for (int p = lane; p < 64; p += 32) {
         const int32_t n1 = atomicExch(&dn->noise[1][p], 0);
         const int32_t n0 = atomicExch(&dn->noise[0][p], 0);
-        dn->offset[1][p] = (cnt1 * dn->denoise + n1 / 2) / (n1 + 1);
-        dn->offset[0][p] = (cnt0 * dn->denoise + n0 / 2) / (n0 + 1);
+        const int u = p & 7, v = p >> 3;
+        /* the reference keeps Int32 offsets and loads them as UInt16 */
+        dn->offset[1][u][v] = (uint16_t)((cnt1 * dn->denoise + n1 / 2) / (n1 + 1));
+        dn->offset[0][u][v] = (uint16_t)((cnt0 * dn->denoise + n0 / 2) / (n0 + 1));
     }
     __threadfence();
     if (lane == 0)
         atomicExch(&dn->ticket, 0u);
 }
 
+/* publish a warp's statistics for a run of n MBs of one session and type;
+ * the publication that completes the session's frame updates the offsets */
+__device__ __forceinline__ void publish_run(const h261b_session_dev_t &S, int t, int n, const int32_t colsum[8],
+                                            int lane)
+{
+    h261b_denoise_dev_t *dn = S.dn;
+    if (lane < 8) {
+#pragma unroll
+        for (int v = 0; v < 8; v++)
+            if (colsum[v])
+                atomicAdd(&dn->noise[t][v * 8 + lane], colsum[v]);
+    }
+    if (lane == 0)
+        atomicAdd(&dn->count[t], 6 * n);
+    __threadfence();
+    __syncwarp();
+    uint32_t last = 0;
+    if (lane == 0)
+        last = atomicAdd(&dn->ticket, (uint32_t)n) + (uint32_t)n == (uint32_t)(S.mbw * S.mbh) ? 1u : 0u;
+    last = __shfl_sync(FULL, last, 0);
+    if (last) {
+        __threadfence();
+        denoise_frame_end(dn, lane);
+    }
+}
+
 template <int FMAD>
 __global__ void __launch_bounds__(256) step_kernel(const h261b_session_dev_t *__restrict__ sessions,
-                                                   const uint32_t *__restrict__ work, int32_t n_work,
+                                                   const uint32_t *__restrict__ work, int32_t n_work, int32_t chunk,
                                                    int32_t phases)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    WarpSmem &s = reinterpret_cast<WarpSmem *>(smem_raw)[warp];
+    WarpSmem &sm = reinterpret_cast<WarpSmem *>(smem_raw)[warp];
     const int warps = blockDim.x >> 5;
+    const int begin = (blockIdx.x * warps + warp) * chunk;
+    const int end = min(begin + chunk, n_work);
+    if (begin >= end)
+        return;
+    const bool want_enc = (phases & H261B_PHASE_ENCDEC) != 0;
 
-    for (int g = blockIdx.x * warps + warp; g < n_work; g += gridDim.x * warps) {
-        const uint32_t item = work[g];
+    {
+        const uint32_t item = work[begin];
         const h261b_session_dev_t &S = sessions[item >> 12];
+        const int mb = (int)(item & 0xFFFu), mby = mb / S.mbw;
+        stage_mb(sm.buf[0], S, mb - mby * S.mbw, mby, lane);
+        cp_async_commit();
+    }
+
+    int run_s = -1, run_t = 0, run_n = 0;
+    int32_t colsum[8];
+#pragma unroll
+    for (int v = 0; v < 8; v++)
+        colsum[v] = 0;
+
+    for (int g = begin; g < end; g++) {
+        const int cur = (g - begin) & 1;
+        if (g + 1 < end) {
+            const uint32_t nitem = work[g + 1];
+            const h261b_session_dev_t &N = sessions[nitem >> 12];
+            const int nmb = (int)(nitem & 0xFFFu), nmby = nmb / N.mbw;
+            stage_mb(sm.buf[cur ^ 1], N, nmb - nmby * N.mbw, nmby, lane);
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncwarp();
+
+        const uint32_t item = work[g];
+        const int sidx = (int)(item >> 12);
+        const h261b_session_dev_t &S = sessions[sidx];
         const int mb = (int)(item & 0xFFFu);
         const int mby = mb / S.mbw, mbx = mb - mby * S.mbw;
+        const StageBuf &b = sm.buf[cur];
         const bool do_me = (phases & H261B_PHASE_ME) && !S.skip_search;
-        const bool do_enc = (phases & H261B_PHASE_ENCDEC) != 0;
-        load_sources(s, S, mbx, mby, lane, do_me || do_enc);
 
         me_gpu_mb_t me;
         me.i_intra_cost = me.i_zero_cost = me.i_16x16_cost = me.i_16x16_filter_cost = 0;
         me.s_16x16_mv.i8_mx = me.s_16x16_mv.i8_my = 0;
         int8_t s1x = 0, s1y = 0;
         if (do_me) {
-            motion_estimate(s, S, mbx, mby, lane, me, s1x, s1y);
+            motion_estimate(b, S, mbx, mby, lane, me, s1x, s1y);
             if (lane == 0) {
                 if (S.me_out)
                     S.me_out[mb] = me;
@@ -707,8 +841,12 @@ __global__ void __launch_bounds__(256) step_kernel(const h261b_session_dev_t *__
                 int32_t d[16];
                 const int sb = lane & 15;
 #pragma unroll
-                for (int k = 0; k < 16; k++)
-                    d[k] = cur_byte(s, (sb >> 2) * 4 + (k >> 2), (sb & 3) * 4 + (k & 3));
+                for (int iy = 0; iy < 4; iy++) {
+                    const uint32_t cw = b.cur[((sb >> 2) * 4 + iy) * 4 + (sb & 3)];
+#pragma unroll
+                    for (int ix = 0; ix < 4; ix++)
+                        d[iy * 4 + ix] = (int32_t)((cw >> (8 * ix)) & 0xFFu);
+                }
                 const int32_t v = satd4x4(d);
                 me.i_intra_cost = (int32_t)__reduce_add_sync(FULL, lane < 16 ? (uint32_t)v : 0u);
             }
@@ -735,18 +873,24 @@ __global__ void __launch_bounds__(256) step_kernel(const h261b_session_dev_t *__
             m.flags = m.mvx = m.mvy = m.cost = 0;
         }
 
-        if (do_enc) {
+        if (want_enc) {
+            const int t = m.type == H261B_MB_TYPE_INTRA ? 0 : 1;
+            if (run_n > 0 && (sidx != run_s || t != run_t)) {
+                publish_run(sessions[run_s], run_t, run_n, colsum, lane);
+                run_n = 0;
+#pragma unroll
+                for (int v = 0; v < 8; v++)
+                    colsum[v] = 0;
+            }
+            run_s = sidx;
+            run_t = t;
             int quant = S.quant;
             if (S.md_in && !(phases & H261B_PHASE_MD))
                 quant += S.md_in[mb].i_quantiser_adjust;
             quant = min(31, max(1, quant)); /* gpu_device.cu:625-627 */
-            int32_t stat[8];
-#pragma unroll
-            for (int v = 0; v < 8; v++)
-                stat[v] = 0;
-            uint32_t cbp = 0;
-            encdec_pass<FMAD>(s, S, mb, mbx, mby, m, quant, true, lane, stat, cbp);
-            encdec_pass<FMAD>(s, S, mb, mbx, mby, m, quant, false, lane, stat, cbp);
+            uint32_t cbp = encdec_pass<FMAD>(sm.t, b, S, mb, mbx, mby, m, quant, true, lane, colsum);
+            cbp |= encdec_pass<FMAD>(sm.t, b, S, mb, mbx, mby, m, quant, false, lane, colsum);
+            run_n++;
 
             const int flags = m.flags | (cbp ? H261B_MB_COEFF : 0);
             if (lane == 0) {
@@ -775,29 +919,11 @@ __global__ void __launch_bounds__(256) step_kernel(const h261b_session_dev_t *__
                     S.info_out[mb] = inf;
                 }
             }
-            /* publish this MB's denoise statistics, then take a ticket */
-            h261b_denoise_dev_t *dn = S.dn;
-            const int t = m.type == H261B_MB_TYPE_INTRA ? 0 : 1;
-            if (lane < 8) {
-#pragma unroll
-                for (int v = 0; v < 8; v++)
-                    atomicAdd(&dn->noise[t][v * 8 + lane], stat[v]);
-            }
-            if (lane == 0)
-                atomicAdd(&dn->count[t], 6);
-            __threadfence();
-            __syncwarp();
-            uint32_t last = 0;
-            if (lane == 0)
-                last = atomicAdd(&dn->ticket, 1u) == (uint32_t)(S.mbw * S.mbh - 1) ? 1u : 0u;
-            last = __shfl_sync(FULL, last, 0);
-            if (last) {
-                __threadfence();
-                denoise_frame_end(dn, lane);
-            }
         }
-        __syncwarp();
+        __syncwarp(); /* this buffer may be refilled from the next iteration on */
     }
+    if (want_enc && run_n > 0)
+        publish_run(sessions[run_s], run_t, run_n, colsum, lane);
 }
 
 } // namespace
@@ -821,18 +947,48 @@ extern "C" int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const 
         return 0;
     if (warps_per_cta < 1 || warps_per_cta > 8)
         return (int)cudaErrorInvalidValue;
-    const int threads = warps_per_cta * 32;
-    const size_t smem = sizeof(WarpSmem) * (size_t)warps_per_cta;
-    int ctas = (n_work + warps_per_cta - 1) / warps_per_cta;
-    if (max_ctas > 0 && ctas > max_ctas)
-        ctas = max_ctas;
     const int fmad = (phases >> 8) & 1;
     const int ph = phases & 0xFF;
+    const int threads = warps_per_cta * 32;
+    const size_t smem = sizeof(WarpSmem) * (size_t)warps_per_cta;
+    /* one wave of resident CTAs, each warp a contiguous run of work items */
+    static std::mutex mu;
+    static int sms[64], resident[64][2][9];
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess || dev < 0 || dev >= 64)
+        return (int)(err != cudaSuccess ? err : cudaErrorInvalidDevice);
+    int per_sm = 0, nsm = 0;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (!sms[dev]) {
+            if ((err = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+                return (int)err;
+            const int max_smem = (int)(sizeof(WarpSmem) * 8);
+            if ((err = cudaFuncSetAttribute(step_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)) ||
+                (err = cudaFuncSetAttribute(step_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)))
+                return (int)err;
+        }
+        int &r = resident[dev][fmad][warps_per_cta];
+        if (!r) {
+            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, fmad ? step_kernel<1> : step_kernel<0>, threads,
+                                                                smem);
+            if (err != cudaSuccess)
+                return (int)err;
+            r = r < 1 ? 1 : r;
+        }
+        per_sm = r;
+        nsm = sms[dev];
+    }
+    int ctas = max_ctas > 0 ? max_ctas : nsm * per_sm;
+    const long long total_warps = (long long)ctas * warps_per_cta;
+    const int chunk = (int)((n_work + total_warps - 1) / total_warps);
+    ctas = (n_work + chunk * warps_per_cta - 1) / (chunk * warps_per_cta);
     cudaStream_t st = (cudaStream_t)stream;
     if (fmad)
-        step_kernel<1><<<ctas, threads, smem, st>>>(sessions_dev, work_dev, n_work, ph);
+        step_kernel<1><<<ctas, threads, smem, st>>>(sessions_dev, work_dev, n_work, chunk, ph);
     else
-        step_kernel<0><<<ctas, threads, smem, st>>>(sessions_dev, work_dev, n_work, ph);
+        step_kernel<0><<<ctas, threads, smem, st>>>(sessions_dev, work_dev, n_work, chunk, ph);
     return (int)cudaGetLastError();
 }
 

@@ -104,11 +104,13 @@ extern "C" int h261b_encode_picture_noalloc(const h261b_noalloc_picture_t *p, vo
         set_error("h261b_encode_picture_noalloc: QUANT, picture type, search mode or denoise out of range");
         return H261B_ERR_ARG;
     }
-    const uintptr_t a16 = (uintptr_t)p->cur_y | (uintptr_t)p->ref_y | (uintptr_t)p->rec_y;
+    const uintptr_t a16 = (uintptr_t)p->cur_y | (uintptr_t)p->ref_y | (uintptr_t)p->rec_y | (uintptr_t)p->state |
+                          (uintptr_t)p->mbs;
     const uintptr_t a8 = (uintptr_t)p->cur_cb | (uintptr_t)p->cur_cr | (uintptr_t)p->ref_cb | (uintptr_t)p->ref_cr |
-                         (uintptr_t)p->rec_cb | (uintptr_t)p->rec_cr | (uintptr_t)p->state;
+                         (uintptr_t)p->rec_cb | (uintptr_t)p->rec_cr | (uintptr_t)p->levels;
     if ((a16 & 15) || (a8 & 7)) {
-        set_error("h261b_encode_picture_noalloc: luma planes must be 16-byte, chroma planes and state 8-byte aligned");
+        set_error("h261b_encode_picture_noalloc: luma planes, state and results must be 16-byte, chroma planes and "
+                  "levels 8-byte aligned");
         return H261B_ERR_ARG;
     }
     int dev = 0;

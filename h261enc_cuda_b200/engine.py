@@ -21,7 +21,7 @@ class FrameResult:
     frame_type: int
     quant: int
     mbs: np.ndarray        # RESULT_DTYPE[num_mb]
-    levels: np.ndarray     # int8 [num_mb, 6, 64]
+    levels: np.ndarray     # int8 [num_mb, 6, 64], per block column-major (u * 8 + v)
 
     def to_abi(self, width: int) -> np.ndarray:
         """The reference's h261_macroblock_t array for this picture."""
@@ -32,9 +32,11 @@ class FrameResult:
         out["mv"][:, 0] = self.mbs["mvx"]
         out["mv"][:, 1] = self.mbs["mvy"]
         out["cbp"] = self.mbs["cbp"].astype(np.uint8)
-        tc = self.levels.astype(np.int32)
+        n = self.mbs.size
+        raster = self.levels.reshape(n, 6, 8, 8).transpose(0, 1, 3, 2).reshape(n, 6, 64)
+        tc = raster.astype(np.int32)
         intra = self.mbs["type"] == _lib.MB_TYPE_INTRA
-        tc[intra, :, 0] = self.levels[intra, :, 0].view(np.uint8)
+        tc[intra, :, 0] = raster[intra, :, 0].view(np.uint8)
         out["tcoeff"] = tc
         mbw = width // 16
         idx = np.arange(self.mbs.size)
@@ -45,12 +47,14 @@ class FrameResult:
 
 class Engine:
     def __init__(self, device: int = 0, max_sessions: int = 4096, hbm_budget_bytes: int = 0,
-                 me_mode: int = 0, fmad: int = 1, warps_per_cta: int = 0, max_ctas: int = 0):
+                 me_mode: int = 0, fmad: int = 1, warps_per_cta: int = 0, max_ctas: int = 0,
+                 copy_threads: int = 0):
         lib = _lib.core()
         cfg = _lib.EngineConfig()
         lib.h261b_engine_config_default(ctypes.byref(cfg))
         cfg.device, cfg.max_sessions, cfg.hbm_budget_bytes = device, max_sessions, hbm_budget_bytes
         cfg.me_mode, cfg.fmad, cfg.warps_per_cta, cfg.max_ctas = me_mode, fmad, warps_per_cta, max_ctas
+        cfg.copy_threads = copy_threads
         h = ctypes.c_void_p()
         check(lib.h261b_engine_create(ctypes.byref(cfg), ctypes.byref(h)), "h261b_engine_create")
         self._h = h
@@ -77,6 +81,66 @@ class Engine:
         check(_lib.core().h261b_session_submit_device(self._h, sid, ctypes.c_void_p(y_ptr), ctypes.c_void_p(cb_ptr),
                                                       ctypes.c_void_p(cr_ptr), quant), "h261b_session_submit_device")
 
+    def input(self, sid: int, quant: int = 0):
+        """Queue the session's next picture in place: returns writable numpy
+        views (y, cb, cr) of the pinned staging arena; fill them before the
+        next ``step()``."""
+        w, h = self._dims[sid]
+        py, pcb, pcr = (ctypes.POINTER(ctypes.c_uint8)() for _ in range(3))
+        check(_lib.core().h261b_session_input(self._h, sid, quant, ctypes.byref(py), ctypes.byref(pcb),
+                                              ctypes.byref(pcr)), "h261b_session_input")
+        ny = w * h
+        return (np.ctypeslib.as_array(py, shape=(ny,)), np.ctypeslib.as_array(pcb, shape=(ny // 4,)),
+                np.ctypeslib.as_array(pcr, shape=(ny // 4,)))
+
+    def inputs(self, sids, quants=None):
+        """Queue the next picture of many sessions in one call: returns the
+        pinned staging arena as a writable uint8 array and an int64 array
+        (n, 3) of the Y, Cb, Cr plane offsets of each session in it."""
+        sids = np.ascontiguousarray(sids, np.int32)
+        n = sids.size
+        q = None if quants is None else np.ascontiguousarray(quants, np.int32)
+        offs = np.empty((n, 3), np.int64)
+        base = ctypes.c_void_p()
+        check(_lib.core().h261b_engine_inputs(self._h, n, sids.ctypes.data, None if q is None else q.ctypes.data,
+                                              ctypes.byref(base), offs.ctypes.data), "h261b_engine_inputs")
+        if n == 0:
+            return np.empty(0, np.uint8), offs
+        w, h = self._dims[int(sids[int(np.argmax(offs[:, 0]))])]
+        size = int(offs[:, 0].max()) + w * h * 3 // 2 + 512
+        arena = np.ctypeslib.as_array((ctypes.c_uint8 * size).from_address(base.value))
+        return arena, offs
+
+    def submit_batch(self, sids, y_ptrs, cb_ptrs, cr_ptrs, quants=None) -> None:
+        """Queue one host picture for each of ``sids``: plane addresses as
+        uint64 arrays (packed planes, e.g. ``frame.ctypes.data`` and the
+        offsets of Cb and Cr in it).  The engine's copy threads move the
+        pictures into the staging arena before the call returns."""
+        sids = np.ascontiguousarray(sids, np.int32)
+        ptrs = [np.ascontiguousarray(a, np.uint64) for a in (y_ptrs, cb_ptrs, cr_ptrs)]
+        q = None if quants is None else np.ascontiguousarray(quants, np.int32)
+        check(_lib.core().h261b_engine_submit_batch(self._h, sids.size, sids.ctypes.data, ptrs[0].ctypes.data,
+                                                    ptrs[1].ctypes.data, ptrs[2].ctypes.data,
+                                                    None if q is None else q.ctypes.data),
+              "h261b_engine_submit_batch")
+
+    def submit_frames(self, sids, frames, quants=None) -> None:
+        """``submit_batch`` for packed frames (uint8 arrays of W*H*3/2)."""
+        y = np.array([f.ctypes.data for f in frames], np.uint64)
+        ny = np.array([self._dims[int(s)][0] * self._dims[int(s)][1] for s in sids], np.uint64)
+        self.submit_batch(sids, y, y + ny, y + ny + ny // 4, quants)
+
+    def step_records(self):
+        """(step number, MB records of every session that step encoded) for
+        the latest completed step; a view valid until the step after next."""
+        ptr, count, step = ctypes.c_void_p(), ctypes.c_int64(), ctypes.c_int64()
+        check(_lib.core().h261b_engine_step_records(self._h, ctypes.byref(ptr), ctypes.byref(count),
+                                                    ctypes.byref(step)), "h261b_engine_step_records")
+        if count.value == 0:
+            return step.value, np.empty(0, _lib.RESULT_DTYPE)
+        buf = (ctypes.c_uint8 * (count.value * 16)).from_address(ptr.value)
+        return step.value, np.ctypeslib.as_array(buf).view(_lib.RESULT_DTYPE)
+
     def submit_frame(self, sid: int, frame: np.ndarray, quant: int = 0) -> None:
         w, h = self._dims[sid]
         fs = w * h
@@ -88,6 +152,10 @@ class Engine:
 
     def sync(self) -> None:
         check(_lib.core().h261b_engine_sync(self._h), "h261b_engine_sync")
+
+    def wait_previous(self) -> None:
+        """Wait for the step before the last one issued."""
+        check(_lib.core().h261b_engine_wait_previous(self._h), "h261b_engine_wait_previous")
 
     def result(self, sid: int, copy: bool = True) -> FrameResult:
         r = _lib.FrameResult()
@@ -112,6 +180,13 @@ class Engine:
         ms = ctypes.c_float()
         check(_lib.core().h261b_engine_last_kernel_ms(self._h, ctypes.byref(ms)), "h261b_engine_last_kernel_ms")
         return ms.value
+
+    def last_copy_bytes(self):
+        """(host-to-device, device-to-host) bytes the last step copied."""
+        a, b = ctypes.c_int64(), ctypes.c_int64()
+        check(_lib.core().h261b_engine_last_copy_bytes(self._h, ctypes.byref(a), ctypes.byref(b)),
+              "h261b_engine_last_copy_bytes")
+        return a.value, b.value
 
     def stats(self):
         o, q, b = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()

@@ -6,10 +6,12 @@
  *      points, one process-global encoder, synchronous calls);
  *   2. this batched engine: many independent encode sessions of mixed size
  *      and QUANT share one device; each h261b_engine_step() encodes the next
- *      picture of every session that has one queued, in one launch (one CUDA
- *      graph replay) over a flat macroblock work list.  Source pictures go up
+ *      picture of every session that has one queued, in one launch over a
+ *      flat macroblock work list.  Source pictures go up
  *      in one host-to-device copy per step, compact results come back in one
- *      copy, reconstructions stay in HBM as the next reference.
+ *      copy, reconstructions stay in HBM as the next reference.  Steps
+ *      alternate between two streams so that one step's copies overlap the
+ *      neighbouring steps' kernels.
  *
  * All functions return H261B_OK (0) or a negative status; the text of the
  * last failure on the calling thread is available from h261b_last_error().
@@ -56,7 +58,9 @@ typedef struct {
                                  defaults), 0: separately rounded            */
     int32_t warps_per_cta;    /* 1..8, 0 = tuned                              */
     int32_t max_ctas;         /* grid cap, 0 = one wave of resident CTAs     */
-    int32_t use_graphs;       /* 1: replay each step from a CUDA graph       */
+    int32_t copy_threads;     /* host threads copying batched submissions
+                                 into the staging arena (the caller's thread
+                                 included); 0 = min(8, cores / 2), 1 = none  */
 } h261b_engine_config_t;
 
 void h261b_engine_config_default(h261b_engine_config_t *cfg);
@@ -82,6 +86,29 @@ int h261b_session_close(h261b_engine_t *e, int32_t session_id);
 int h261b_session_submit(h261b_engine_t *e, int32_t session_id, const uint8_t *y, const uint8_t *cb,
                          const uint8_t *cr, int32_t quant);
 
+/* Queue the session's next picture by writing it in place: on return *y,
+ * *cb and *cr point into the pinned staging arena (packed planes, strides
+ * W and W/2); fill them before the next h261b_engine_step().  Saves the
+ * copy h261b_session_submit makes. */
+int h261b_session_input(h261b_engine_t *e, int32_t session_id, int32_t quant, uint8_t **y, uint8_t **cb,
+                        uint8_t **cr);
+
+/* h261b_session_input for n sessions in one call.  On return *staging is the
+ * pinned arena the pictures go into and offsets[3i], [3i+1], [3i+2] the byte
+ * offsets of session ids[i]'s Y, Cb and Cr planes in it.  quants may be NULL
+ * (every session keeps its QUANT).  All or nothing: on an error no session
+ * of the call is queued. */
+int h261b_engine_inputs(h261b_engine_t *e, int32_t n, const int32_t *ids, const int32_t *quants,
+                        uint8_t **staging, int64_t *offsets);
+
+/* h261b_session_submit for n sessions in one call: session ids[i] gets the
+ * picture y[i], cb[i], cr[i] (packed planes) and QUANT quants[i] (quants may
+ * be NULL).  The pictures are copied into the staging arena by the engine's
+ * copy threads before the call returns.  All or nothing, as
+ * h261b_engine_inputs. */
+int h261b_engine_submit_batch(h261b_engine_t *e, int32_t n, const int32_t *ids, const uint8_t *const *y,
+                              const uint8_t *const *cb, const uint8_t *const *cr, const int32_t *quants);
+
 /* Queue a picture that is already in device memory (packed planes, pitch W
  * and W/2; Y 16-byte and Cb/Cr 8-byte aligned).  It must stay unchanged
  * until the step that reads it has completed. */
@@ -92,7 +119,11 @@ int h261b_session_submit_device(h261b_engine_t *e, int32_t session_id, const uin
  * Returns the number of pictures encoded (>= 0) or a negative status.  The
  * call is asynchronous; results become readable after h261b_engine_sync(). */
 int h261b_engine_step(h261b_engine_t *e);
+/* Wait for the last step issued / for the one before it (so the host can
+ * read step k's results while step k+1 runs).  A step's results stay
+ * readable until the step after next is issued. */
 int h261b_engine_sync(h261b_engine_t *e);
+int h261b_engine_wait_previous(h261b_engine_t *e);
 
 /* per-macroblock result of a step (16 bytes) */
 typedef struct {
@@ -111,13 +142,23 @@ typedef struct {
     int32_t quant;            /* picture QUANT used                           */
     int32_t num_mb;
     const h261b_mb_result_t *mbs;  /* num_mb entries                          */
-    const int8_t *levels;     /* num_mb x 6 x 64 quantised levels, raster
-                                 order; an intra DC is stored as uint8 1..255 */
+    const int8_t *levels;     /* num_mb x 6 x 64 quantised levels, each
+                                 block column-major (index u * 8 + v for
+                                 horizontal frequency u, vertical v); an
+                                 intra DC is stored as uint8 1..255          */
 } h261b_frame_result_t;
 
-/* Results of the last completed step for a session (pointers stay valid
- * until the next h261b_engine_step()). Requires h261b_engine_sync(). */
+/* Results of the latest completed step that encoded this session (pointers
+ * stay valid until the step after next is issued). */
 int h261b_session_result(h261b_engine_t *e, int32_t session_id, h261b_frame_result_t *out);
+
+/* The macroblock records of the latest completed step as one array: the
+ * records of every session the step encoded, session after session in
+ * ascending session id (each session's h261b_session_result().mbs points
+ * into it).  *step receives the step's number (0, 1, ...), -1 and *count 0
+ * when no step has completed.  Valid until the step after next is issued. */
+int h261b_engine_step_records(h261b_engine_t *e, const h261b_mb_result_t **records, int64_t *count,
+                              int64_t *step);
 
 /* Copy the session's latest reconstruction (packed planes) to the host. */
 int h261b_session_recon(h261b_engine_t *e, int32_t session_id, uint8_t *y, uint8_t *cb, uint8_t *cr);
@@ -128,6 +169,9 @@ int h261b_result_to_abi(const h261b_frame_result_t *r, int32_t width, h261_macro
 
 /* Device time of the last step's kernel in milliseconds (CUDA events). */
 int h261b_engine_last_kernel_ms(h261b_engine_t *e, float *ms);
+/* Bytes the last step copied host->device (descriptors, work list,
+ * pictures) and device->host (records and levels). */
+int h261b_engine_last_copy_bytes(h261b_engine_t *e, int64_t *h2d, int64_t *d2h);
 /* Throughput of the 4-pixel SAD primitive the motion search uses, measured
  * on the device with every SM busy: absolute differences per second. */
 int h261b_measure_sad_peak(int32_t device, double *absdiff_per_s);
@@ -163,7 +207,8 @@ typedef struct {
 } h261b_noalloc_picture_t;
 
 /* Queue the encode of one picture on `stream` (a cudaStream_t, may be 0).
- * Luma planes 16-byte aligned, chroma planes and state 8-byte aligned. */
+ * Luma planes, state and mbs 16-byte aligned; chroma planes and levels
+ * 8-byte aligned. */
 int h261b_encode_picture_noalloc(const h261b_noalloc_picture_t *pic, void *stream);
 
 /* Number of sessions open / queued, device bytes held. */

@@ -69,8 +69,8 @@ def test_result_to_abi_expansion():
     mbs["mvy"] = [0, 5]
     lv = np.zeros((2, 6, 64), np.int8)
     lv[0, :, 0] = np.array([200, 255, 1, 128, 17, 254], np.uint8).view(np.int8)
-    lv[1, 0, 5] = -7
+    lv[1, 0, 5 * 8 + 2] = -7          # column u = 5, row v = 2
     out = FrameResult(0, 0, 8, mbs, lv).to_abi(32)
     assert list(out["tcoeff"][0, :, 0]) == [200, 255, 1, 128, 17, 254]
-    assert out["tcoeff"][1, 0, 5] == -7 and out["mv"][1].tolist() == [-3, 5]
+    assert out["tcoeff"][1, 0, 2 * 8 + 5] == -7 and out["mv"][1].tolist() == [-3, 5]
     assert out["mb_x"].tolist() == [0, 16] and out["cbp"].tolist() == [63, 33]

@@ -1,0 +1,140 @@
+"""The engine's pipelined use: steps issued back to back on its two streams,
+the host reading step k-1 while step k runs, streams ending and new sessions
+taking their place without a drain, and the three ways of queueing host
+pictures (one copy per call, the batched copy, writing in place).  Every
+picture must still be bit-exact to the oracle."""
+import numpy as np
+import pytest
+
+import oracle as O
+from h261enc_cuda_b200 import _lib, synth
+from h261enc_cuda_b200.engine import Engine
+
+pytestmark = pytest.mark.gpu
+
+
+class Instance:
+    """One encode stream: a clip, its oracle output and its session."""
+
+    def __init__(self, w, h, q, n, seed):
+        self.w, self.h, self.q, self.n = w, h, q, n
+        self.clip = synth.clip(2, w, h, seed, n)
+        self.want = O.encode_sequence(self.clip, w, h, q)
+        self.sid = None
+        self.pos = 0        # pictures queued
+        self.seen = 0       # results checked
+
+
+def _check(e, inst, where):
+    r = e.result(inst.sid)
+    assert r.frame_index == inst.seen, f"{where}: frame index {r.frame_index} != {inst.seen}"
+    got = r.to_abi(inst.w)
+    want = inst.want["mbs"][inst.seen]
+    for f in ("type", "flags", "quant", "cbp"):
+        assert np.array_equal(got[f], want[f]), f"{where}: {f} differs"
+    assert np.array_equal(got["mv"], want["mv"]), f"{where}: vectors differ"
+    assert np.array_equal(got["tcoeff"], want["tcoeff"]), f"{where}: levels differ"
+    inst.seen += 1
+    return r.mbs
+
+
+def _queue(e, live, mode):
+    sids = [i.sid for i in live]
+    frames = [i.clip[i.pos] for i in live]
+    if mode == 0:
+        for s, f in zip(sids, frames):
+            e.submit_frame(s, f)
+    elif mode == 1:
+        e.submit_frames(sids, frames)
+    else:
+        arena, offs = e.inputs(sids)
+        for inst, f, o in zip(live, frames, offs):
+            ny = inst.w * inst.h
+            arena[o[0]:o[0] + ny] = f[:ny]
+            arena[o[1]:o[1] + ny // 4] = f[ny:ny + ny // 4]
+            arena[o[2]:o[2] + ny // 4] = f[ny + ny // 4:]
+    for inst in live:
+        inst.pos += 1
+
+
+def test_pipelined_steps_with_turnover_match_oracle(gpu):
+    # (width, height, QUANT, pictures, seed): several short streams per slot
+    slots = [
+        [(176, 144, 8, 3, 21), (176, 144, 10, 4, 22), (176, 144, 6, 5, 23)],
+        [(352, 288, 12, 5, 31), (352, 288, 16, 2, 32), (352, 288, 9, 4, 33)],
+        [(176, 144, 4, 2, 41), (352, 288, 20, 3, 42), (176, 144, 14, 6, 43)],
+        [(176, 144, 24, 7, 51), (176, 144, 2, 3, 52)],
+    ]
+    todo = [[Instance(*spec) for spec in slot] for slot in slots]
+    for k, q in enumerate(todo):
+        for inst in q:
+            inst.slot = k
+    with Engine(warps_per_cta=4, max_sessions=16) as e:
+        live = []
+        for q in todo:
+            inst = q.pop(0)
+            inst.sid = e.open(inst.w, inst.h, inst.q)
+            live.append(inst)
+        prev, closing, step = None, [], 0
+        while live or prev:
+            if live:
+                _queue(e, live, step % 3)
+                assert e.step() == len(live)
+            cur = list(live)
+            # streams whose last picture is now queued make room for the next
+            nxt = []
+            for inst in live:
+                if inst.pos == inst.n:
+                    closing.append(inst)
+                    if todo[inst.slot]:
+                        new = todo[inst.slot].pop(0)
+                        new.sid = e.open(new.w, new.h, new.q)
+                        nxt.append(new)
+                else:
+                    nxt.append(inst)
+            live = nxt
+            if prev is not None:
+                if cur:
+                    e.wait_previous()
+                else:
+                    e.sync()
+                recs = [_check(e, inst, f"step {step - 1} session {inst.sid}") for inst in
+                        sorted(prev, key=lambda i: i.sid)]
+                done, flat = e.step_records()
+                assert done >= step - 1
+                if done == step - 1:
+                    assert np.array_equal(flat, np.concatenate(recs))
+                # a stream is closed once its last picture has been read
+                for inst in [i for i in closing if i.seen == i.n]:
+                    e.close(inst.sid)
+                    closing.remove(inst)
+            prev = cur if cur else None
+            step += 1
+    for slot in todo:
+        assert not slot
+    assert not closing
+
+
+def test_inputs_are_all_or_nothing(gpu):
+    with Engine(warps_per_cta=4) as e:
+        a = e.open(176, 144, 8)
+        b = e.open(352, 288, 8)
+        with pytest.raises(RuntimeError):
+            e.inputs([a, a])
+        with pytest.raises(RuntimeError):
+            e.inputs([a, 99])
+        arena, offs = e.inputs([b, a])     # nothing was left queued
+        assert offs.shape == (2, 3) and offs[1, 0] >= offs[0, 2] + 352 * 288 // 4
+        c = e.open(176, 144, 8)
+        fr = synth.clip(0, 176, 144, 3, 1)[0]
+        with pytest.raises(RuntimeError):
+            e.submit_frames([c, a], [fr, fr])   # a is already queued
+        e.submit_frames([c], [fr])
+        assert e.step() == 3
+        e.sync()
+
+
+def test_step_records_before_any_step(gpu):
+    with Engine(warps_per_cta=4) as e:
+        step, recs = e.step_records()
+        assert step == -1 and recs.size == 0 and recs.dtype == _lib.RESULT_DTYPE
