@@ -96,6 +96,46 @@ int32_t orc_encode_sequence(const uint8_t *yuv, int32_t w, int32_t h, int32_t nf
                             uint8_t *recon_out, h261_macroblock_t *mbs_out, me_gpu_mb_t *me_out,
                             h261_mb_mode_decision_t *md_out);
 
+/* ---- bitstream syntax and rate control (h261_writer.c) ---- */
+
+/* one picture in H.261 syntax from its macroblock records (QCIF or CIF):
+ * src/h261_picture.c:115-148, src/h261_gob.c:6-199,
+ * src/h261_macroblock.c:5-262.  Returns the byte count, -1 if out_cap is
+ * too small, -2 for another picture size, -3 for records the reference
+ * writer cannot write (it dereferences NULL on those). */
+int32_t orc_write_picture(int32_t w, int32_t h, int32_t frame_num, int32_t frame_type, int32_t quant,
+                          const h261_macroblock_t *mbs, uint8_t *out, int32_t out_cap);
+/* transmission order: raster index of the k-th coefficient sent */
+const uint8_t *orc_zigzag(void);
+
+/* src/h261_ratectrl.c state (h261_ratectrl_t without the mode field) */
+typedef struct {
+    int32_t current_quant;
+    int32_t prediction_cost[2];
+    int32_t prediction_size[2];
+    int32_t bitrate;              /* bytes per second   */
+    int32_t vbv_size;             /* bytes              */
+    int32_t vbv_fill;
+    int32_t current_picture_cost;
+} orc_rc_t;
+
+void orc_rc_init(orc_rc_t *rc, int32_t quant, int32_t bitrate, int32_t vbv_size);
+/* picture QUANT from the mode-decision cost sum (collect_picture_stats +
+ * init_picture + h261_init_picture's clamp) */
+int32_t orc_rc_picture_quant(orc_rc_t *rc, int32_t frame_type, int32_t picture_cost, int32_t num_mb);
+/* after the picture: its QUANT and its size in bytes */
+void orc_rc_update(orc_rc_t *rc, int32_t frame_type, int32_t quant, int32_t bytes);
+
+/* the reference encoder's whole frame loop (h261_main.c:178-275 plus an
+ * intra period): fixed QUANT when quant > 0, else CBR rate control started
+ * at QUANT 10 with VBV = bitrate.  Writes the concatenated pictures to bits
+ * (capacity bits_cap) and per picture its byte count and QUANT; recon_out
+ * optional.  Returns the total byte count, or a negative status. */
+int64_t orc_encode_stream(const uint8_t *yuv, int32_t w, int32_t h, int32_t nframes, int32_t quant,
+                          int32_t bitrate, int32_t intra_period, int32_t denoise, int32_t fmad,
+                          int32_t me_mode, uint8_t *bits, int64_t bits_cap, int32_t *frame_bytes,
+                          int32_t *frame_quant, uint8_t *recon_out);
+
 #ifdef __cplusplus
 }
 #endif

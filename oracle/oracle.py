@@ -64,6 +64,16 @@ def lib() -> ctypes.CDLL:
         L.orc_encode_sequence.argtypes = [c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_int32,
                                           c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_void_p]
         L.orc_encode_sequence.restype = c_int32
+        L.orc_write_picture.argtypes = [c_int32] * 5 + [c_void_p, c_void_p, c_int32]
+        L.orc_write_picture.restype = c_int32
+        L.orc_zigzag.restype = POINTER(c_uint8)
+        L.orc_encode_stream.argtypes = [c_void_p] + [c_int32] * 9 + [c_void_p, ctypes.c_int64, c_void_p,
+                                                                        c_void_p, c_void_p]
+        L.orc_encode_stream.restype = ctypes.c_int64
+        L.orc_rc_init.argtypes = [c_void_p, c_int32, c_int32, c_int32]
+        L.orc_rc_picture_quant.argtypes = [c_void_p, c_int32, c_int32, c_int32]
+        L.orc_rc_picture_quant.restype = c_int32
+        L.orc_rc_update.argtypes = [c_void_p, c_int32, c_int32, c_int32]
         _lib = L
     return _lib
 
@@ -111,6 +121,60 @@ def encode_sequence(frames: np.ndarray, width: int, height: int, quant: int, int
     if rc < 0:
         raise ValueError("orc_encode_sequence: bad arguments")
     return {"recon": recon, "mbs": mbs, "me": me, "md": md}
+
+
+def write_picture_oracle(mbs: np.ndarray, width: int, height: int, frame_num: int, frame_type: int,
+                         quant: int) -> bytes:
+    """H.261 bytes of one picture from h261_macroblock_t records, written by
+    the oracle's restatement of the reference writers (h261_writer.c)."""
+    m = np.ascontiguousarray(mbs, MB_DTYPE)
+    buf = np.zeros(400 * 1024, np.uint8)
+    n = lib().orc_write_picture(width, height, frame_num, frame_type, quant, _p(m), _p(buf), buf.size)
+    if n < 0:
+        raise ValueError(f"orc_write_picture: status {n}")
+    return buf[:n].tobytes()
+
+
+def zigzag() -> np.ndarray:
+    """Transmission order: raster index (row = vertical frequency) of the
+    k-th coefficient sent."""
+    return np.ctypeslib.as_array(lib().orc_zigzag(), shape=(64,)).copy()
+
+
+def encode_stream(frames: np.ndarray, width: int, height: int, quant: int = 0, bitrate: int = 384000,
+                  intra_period: int = 0, denoise: int = 5, fmad: int = 1, me_mode: int = 0):
+    """The reference's frame loop with its bitstream: fixed QUANT, or CBR
+    rate control when quant == 0.  Returns (bytes, per-picture byte counts,
+    per-picture QUANT, reconstructions)."""
+    n = frames.shape[0]
+    fr = np.ascontiguousarray(frames, np.uint8)
+    recon = np.zeros_like(fr)
+    cap = n * 400 * 1024
+    bits = np.zeros(cap, np.uint8)
+    nb = np.zeros(n, np.int32)
+    nq = np.zeros(n, np.int32)
+    total = lib().orc_encode_stream(_p(fr), width, height, n, quant, bitrate, intra_period, denoise, fmad,
+                                    me_mode, _p(bits), cap, _p(nb), _p(nq), _p(recon))
+    if total < 0:
+        raise ValueError(f"orc_encode_stream: status {total}")
+    return bits[:total].tobytes(), nb, nq, recon
+
+
+class RateControl:
+    """The oracle's restatement of the reference rate control."""
+
+    def __init__(self, quant: int = 10, bitrate: int = 384000, vbv: int | None = None):
+        self._s = (c_int32 * 9)()
+        lib().orc_rc_init(ctypes.byref(self._s), quant, bitrate, bitrate if vbv is None else vbv)
+
+    def picture_quant(self, frame_type: int, picture_cost: int, num_mb: int) -> int:
+        return lib().orc_rc_picture_quant(ctypes.byref(self._s), frame_type, picture_cost, num_mb)
+
+    def update(self, frame_type: int, quant: int, nbytes: int) -> None:
+        lib().orc_rc_update(ctypes.byref(self._s), frame_type, quant, nbytes)
+
+    def state(self):
+        return list(self._s)
 
 
 def me_frame(cur_y: np.ndarray, ref_y: np.ndarray, width: int, height: int, mode: int = 0):
