@@ -53,7 +53,7 @@ MB_DTYPE = np.dtype([("addr", "<i4"), ("type", "<i4"), ("flags", "<i4"), ("quant
                      ("mv", "<i4", 2), ("cbp", "<i4"), ("tcoeff", "<i4", (6, 64)),
                      ("mb_x", "<i4"), ("mb_y", "<i4")])
 RESULT_DTYPE = np.dtype([("type", "<i2"), ("flags", "<i2"), ("quant", "i1"), ("cbp", "i1"),
-                         ("mvx", "i1"), ("mvy", "i1"), ("cost", "<i4"), ("reserved", "<i4")])
+                         ("mvx", "i1"), ("mvy", "i1"), ("cost", "<i4"), ("coef_bits", "<i4")])
 assert ME_MB_DTYPE.itemsize == 20 and MD_DTYPE.itemsize == 24 and MB_DTYPE.itemsize == 1572
 assert RESULT_DTYPE.itemsize == 16
 
@@ -61,17 +61,19 @@ assert RESULT_DTYPE.itemsize == 16
 class EngineConfig(Structure):
     _fields_ = [("device", c_int32), ("max_sessions", c_int32), ("hbm_budget_bytes", c_int64),
                 ("me_mode", c_int32), ("fmad", c_int32), ("warps_per_cta", c_int32),
-                ("max_ctas", c_int32), ("copy_threads", c_int32)]
+                ("max_ctas", c_int32), ("copy_threads", c_int32), ("levels_to_host", c_int32),
+                ("bits_host_bytes", c_int64)]
 
 
 class SessionConfig(Structure):
     _fields_ = [("width", c_int32), ("height", c_int32), ("quant", c_int32),
-                ("intra_period", c_int32), ("denoise", c_int32)]
+                ("intra_period", c_int32), ("denoise", c_int32), ("bitstream", c_int32)]
 
 
 class FrameResult(Structure):
     _fields_ = [("frame_index", c_int32), ("frame_type", c_int32), ("quant", c_int32),
-                ("num_mb", c_int32), ("mbs", c_void_p), ("levels", POINTER(c_int8))]
+                ("num_mb", c_int32), ("mbs", c_void_p), ("levels", POINTER(c_int8)),
+                ("bits", c_void_p), ("bits_bytes", c_int32), ("bits_status", c_int32)]
 
 
 class SynthParams(Structure):
@@ -115,6 +117,9 @@ def core() -> ctypes.CDLL:
                                             POINTER(POINTER(c_uint8)), POINTER(POINTER(c_uint8))]
         lib.h261b_engine_submit_batch.argtypes = [c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
                                                   c_void_p]
+        lib.h261b_engine_step_bits.argtypes = [c_void_p, POINTER(ctypes.c_int64), POINTER(c_int32)]
+        lib.h261b_session_bits_bytes.argtypes = [c_int32, c_int32]
+        lib.h261b_session_bits_bytes.restype = c_int64
         lib.h261b_engine_last_copy_bytes.argtypes = [c_void_p, POINTER(ctypes.c_int64), POINTER(ctypes.c_int64)]
         lib.h261b_engine_inputs.argtypes = [c_void_p, c_int32, c_void_p, c_void_p, POINTER(c_void_p), c_void_p]
         lib.h261b_engine_step_records.argtypes = [c_void_p, POINTER(c_void_p), POINTER(ctypes.c_int64),

@@ -134,6 +134,43 @@ struct Result {
     int64_t step = -1;
     int32_t frame = 0, type = 0, quant = 0;
     size_t info_off = 0, level_off = 0;
+    size_t pic_off = 0;            /* h261b_pic_info_t of a bitstream session */
+    bool has_bits = false;
+};
+
+/* pinned host memory the device writes into (mapped) */
+struct HostArena {
+    uint8_t *host = nullptr;
+    uint8_t *dev = nullptr;
+    size_t cap = 0;
+    int reserve(size_t bytes)
+    {
+        if (bytes <= cap)
+            return H261B_OK;
+        release();
+        uint8_t *h = nullptr;
+        void *d = nullptr;
+        cudaError_t err = cudaHostAlloc(&h, bytes, cudaHostAllocMapped);
+        if (err == cudaSuccess)
+            err = cudaHostGetDevicePointer(&d, h, 0);
+        if (err != cudaSuccess) {
+            if (h)
+                cudaFreeHost(h);
+            set_error("host bitstream arena of %zu bytes: %s", bytes, cudaGetErrorString(err));
+            return H261B_ERR_NOMEM;
+        }
+        host = h;
+        dev = (uint8_t *)d;
+        cap = bytes;
+        return H261B_OK;
+    }
+    void release()
+    {
+        if (host)
+            cudaFreeHost(host);
+        host = dev = nullptr;
+        cap = 0;
+    }
 };
 
 struct Session {
@@ -146,6 +183,11 @@ struct Session {
     int rec_cur = 0;               /* holds the latest reconstruction     */
     h261b_denoise_dev_t *dn = nullptr;
     size_t slot_bytes = 0;
+    /* bitstream: one device slot per step parity */
+    bool bitstream = false;
+    uint32_t *bits_slot[2] = { nullptr, nullptr };
+    size_t bits_slot_bytes = 0;
+    std::vector<uint8_t> bits_spill;   /* a picture the host arena missed */
     /* queued picture: in the upload arena, or already in device memory */
     bool queued = false;
     size_t src_off = 0;
@@ -181,6 +223,8 @@ struct h261b_engine_s {
     bool in_flight[2] = { false, false };
     int64_t step_mbs[2] = { 0, 0 };   /* MB records of the step in each arena */
     int64_t last_h2d = 0, last_d2h = 0;  /* bytes copied by the last step */
+    HostArena bits[2];         /* pictures written by the bitstream kernel */
+    size_t bits_want = 0;      /* capacity the arenas grow to              */
     /* slots of closed sessions, returned to the pool once the last step
      * that may use them (second field) has completed */
     struct Retired {
@@ -216,6 +260,8 @@ extern "C" void h261b_engine_config_default(h261b_engine_config_t *c)
     c->warps_per_cta = 0;
     c->max_ctas = 0;
     c->copy_threads = 0;
+    c->levels_to_host = 1;
+    c->bits_host_bytes = 0;
 }
 
 extern "C" int64_t h261b_session_bytes(int32_t w, int32_t h)
@@ -223,6 +269,11 @@ extern "C" int64_t h261b_session_bytes(int32_t w, int32_t h)
     if (w < 16 || h < 16 || (w & 15) || (h & 15))
         return -1;
     return (int64_t)(2 * PictureLayout::of(w, h).bytes + align_up(sizeof(h261b_denoise_dev_t), 256));
+}
+
+extern "C" int64_t h261b_session_bits_bytes(int32_t w, int32_t h)
+{
+    return 2 * (int64_t)align_up((size_t)h261b_bits_slot_bytes(w, h), 256);
 }
 
 /* return retired session slots whose last step has completed */
@@ -252,7 +303,7 @@ extern "C" int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engin
     clear_error();
     if (!cfg || !out || cfg->max_sessions < 1 || cfg->max_sessions > 65536 || cfg->warps_per_cta < 0 ||
         cfg->warps_per_cta > 8 || (cfg->me_mode != 0 && cfg->me_mode != 1) || cfg->copy_threads < 0 ||
-        cfg->copy_threads > 64) {
+        cfg->copy_threads > 64 || cfg->bits_host_bytes < 0 || (cfg->levels_to_host != 0 && cfg->levels_to_host != 1)) {
         set_error("h261b_engine_create: bad configuration");
         return H261B_ERR_ARG;
     }
@@ -266,6 +317,7 @@ extern "C" int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engin
     h261b_engine_t *e = new h261b_engine_s();
     e->cfg = *cfg;
     e->sessions.resize((size_t)cfg->max_sessions);
+    e->bits_want = cfg->bits_host_bytes > 0 ? align_up((size_t)cfg->bits_host_bytes, 4096) : (size_t)8 << 20;
     int copiers = cfg->copy_threads;
     if (copiers == 0)
         copiers = std::max(1, std::min(8, (int)std::thread::hardware_concurrency() / 2));
@@ -312,6 +364,7 @@ extern "C" int h261b_engine_destroy(h261b_engine_t *e)
         e->upload[p].release();
         e->results[p].release();
         e->desc[p].release();
+        e->bits[p].release();
         cudaEventDestroy(e->h2d_done[p]);
         cudaEventDestroy(e->kernel_done[p]);
         cudaEventDestroy(e->step_done[p]);
@@ -338,11 +391,17 @@ extern "C" int h261b_session_open(h261b_engine_t *e, const h261b_session_config_
     clear_error();
     if (!e || !c || !id || c->width < 16 || c->height < 16 || (c->width & 15) || (c->height & 15) ||
         (c->width / 16) * (c->height / 16) > H261B_MAX_MB_PER_SESSION || c->quant < 1 || c->quant > 31 ||
-        c->intra_period < 0 || c->denoise < 0) {
+        c->intra_period < 0 || c->denoise < 0 || (c->bitstream != 0 && c->bitstream != 1)) {
         set_error("h261b_session_open: bad session configuration");
         return H261B_ERR_ARG;
     }
-    const int64_t need = h261b_session_bytes(c->width, c->height);
+    const int64_t bits_need = c->bitstream ? h261b_session_bits_bytes(c->width, c->height) : 0;
+    if (c->bitstream && bits_need == 0) {
+        set_error("h261b_session_open: H.261 bitstreams exist for 176x144 and 352x288 only, not %dx%d",
+                  c->width, c->height);
+        return H261B_ERR_ARG;
+    }
+    const int64_t need = h261b_session_bytes(c->width, c->height) + bits_need;
     if (e->cfg.hbm_budget_bytes > 0 && e->session_bytes + need > e->cfg.hbm_budget_bytes) {
         set_error("h261b_session_open: HBM budget %lld exceeded", (long long)e->cfg.hbm_budget_bytes);
         return H261B_ERR_BUDGET;
@@ -378,6 +437,14 @@ extern "C" int h261b_session_open(h261b_engine_t *e, const h261b_session_config_
     s.rec[0] = base;
     s.rec[1] = base + s.lay.bytes;
     s.dn = (h261b_denoise_dev_t *)(base + 2 * s.lay.bytes);
+    if (c->bitstream) {
+        const size_t sb = align_up((size_t)h261b_bits_slot_bytes(c->width, c->height), 256);
+        uint8_t *b0 = base + h261b_session_bytes(c->width, c->height);
+        s.bitstream = true;
+        s.bits_slot_bytes = sb;
+        s.bits_slot[0] = (uint32_t *)b0;
+        s.bits_slot[1] = (uint32_t *)(b0 + sb);
+    }
     /* the first reference is black like the reference's zeroed frame
      * (h261_main.c:155-157); denoise state starts at zero
      * (gpu_device.cu:495-508).  No step in flight touches this slot (a
@@ -425,10 +492,12 @@ static int ensure_capacity(h261b_engine_t *e, int p)
     for (const Session &s : e->sessions)
         if (s.open) {
             up += align_up(s.lay.bytes, 256);
-            res += align_up((size_t)s.nmb * sizeof(h261b_mb_info_t), 256) + align_up((size_t)s.nmb * 384, 256);
+            res += (size_t)s.nmb * sizeof(h261b_mb_info_t) + sizeof(h261b_pic_info_t) +
+                   align_up((size_t)s.nmb * 384, 256);
             n++;
         }
-    const size_t desc = align_up((size_t)n * sizeof(h261b_session_dev_t), 256) +
+    res += 512;   /* alignment of the record, picture and level regions */
+    const size_t desc = sizeof(h261b_step_dev_t) + align_up((size_t)n * sizeof(h261b_session_dev_t), 256) +
                         (size_t)n * H261B_MAX_MB_PER_SESSION * sizeof(uint32_t);
     if (up > e->upload[p].cap || res > e->results[p].cap || desc > e->desc[p].cap) {
         H261B_CUDA_TRY(cudaStreamSynchronize(e->stream[p]));
@@ -666,17 +735,23 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
 
     Mirror &dm = e->desc[p], &rm = e->results[p], &um = e->upload[p];
     const size_t n = list.size();
-    h261b_session_dev_t *desc = (h261b_session_dev_t *)dm.host;
-    const size_t work_off = align_up(n * sizeof(h261b_session_dev_t), 256);
+    /* descriptor arena: step state, session descriptors, work list */
+    memset(dm.host, 0, sizeof(h261b_step_dev_t));
+    const size_t desc_off = sizeof(h261b_step_dev_t);
+    h261b_session_dev_t *desc = (h261b_session_dev_t *)(dm.host + desc_off);
+    const size_t work_off = desc_off + align_up(n * sizeof(h261b_session_dev_t), 256);
     uint32_t *work = (uint32_t *)(dm.host + work_off);
-    /* results arena: the MB records of all sessions back to back, then the
-     * levels of each session on a 256-byte boundary */
+    /* results arena: the MB records of all sessions back to back, the
+     * picture records of the bitstream writer, then the levels of each
+     * session on a 256-byte boundary */
     int64_t total_mb = 0;
     for (int32_t sid : list)
         total_mb += e->sessions[(size_t)sid].nmb;
     size_t info_off = 0;
-    size_t res_off = align_up((size_t)total_mb * sizeof(h261b_mb_info_t), 256);
-    int32_t n_work = 0;
+    const size_t pic_base = align_up((size_t)total_mb * sizeof(h261b_mb_info_t), 256);
+    const size_t levels_base = align_up(pic_base + n * sizeof(h261b_pic_info_t), 256);
+    size_t res_off = levels_base;
+    int32_t n_work = 0, n_bits = 0;
     for (size_t k = 0; k < n; k++) {
         Session &s = e->sessions[(size_t)list[k]];
         if (s.queued_quant > 0)
@@ -722,6 +797,15 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
         r.level_off = res_off;
         d.level_out = (int8_t *)(rm.dev + res_off);
         res_off += align_up((size_t)s.nmb * 384, 256);
+        r.has_bits = s.bitstream;
+        r.pic_off = pic_base + k * sizeof(h261b_pic_info_t);
+        if (s.bitstream) {
+            d.bits_out = s.bits_slot[p];
+            d.bits_cap = (int32_t)s.bits_slot_bytes;
+            d.frame_num = s.frame_index;
+            d.pic_out = (h261b_pic_info_t *)(rm.dev + r.pic_off);
+            n_bits++;
+        }
         for (int32_t m = 0; m < s.nmb; m++)
             work[n_work++] = ((uint32_t)k << 12) | (uint32_t)m;
     }
@@ -739,17 +823,30 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
     const int tuning = next_launch_shape(e, &warps, &ctas);
     H261B_CUDA_TRY(cudaEventRecord(e->k_start[p], st));
     const int phases = H261B_PHASE_ME | H261B_PHASE_MD | H261B_PHASE_ENCDEC | (e->cfg.fmad ? 0x100 : 0);
-    int lr = h261b_launch_step((const h261b_session_dev_t *)dm.dev, (const uint32_t *)(dm.dev + work_off), n_work,
-                               phases, warps, ctas, st);
+    const h261b_session_dev_t *desc_dev = (const h261b_session_dev_t *)(dm.dev + desc_off);
+    int lr = h261b_launch_step(desc_dev, (const uint32_t *)(dm.dev + work_off), n_work, phases, warps, ctas, st);
     if (lr != 0) {
         set_error("step launch failed: %s", cudaGetErrorString((cudaError_t)lr));
         return H261B_ERR_CUDA;
     }
     H261B_CUDA_TRY(cudaEventRecord(e->k_end[p], st));
+    /* the next step may start encoding while this one writes bitstreams */
     H261B_CUDA_TRY(cudaEventRecord(e->kernel_done[p], st));
-    H261B_CUDA_TRY(cudaMemcpyAsync(rm.host, rm.dev, res_off, cudaMemcpyDeviceToHost, st));
+    if (n_bits) {
+        if ((rc = e->bits[p].reserve(e->bits_want)))
+            return rc;
+        lr = h261b_launch_bitstream(desc_dev, (int32_t)n, (h261b_step_dev_t *)dm.dev, e->bits[p].dev,
+                                    (int64_t)e->bits[p].cap, st);
+        if (lr != 0) {
+            set_error("bitstream launch failed: %s", cudaGetErrorString((cudaError_t)lr));
+            return H261B_ERR_CUDA;
+        }
+    }
+    /* records and picture records always, levels when asked for */
+    const size_t d2h = e->cfg.levels_to_host ? res_off : levels_base;
+    H261B_CUDA_TRY(cudaMemcpyAsync(rm.host, rm.dev, d2h, cudaMemcpyDeviceToHost, st));
     e->last_h2d = (int64_t)desc_bytes + (e->upload_checked ? (int64_t)e->upload_used : 0);
-    e->last_d2h = (int64_t)res_off;
+    e->last_d2h = (int64_t)d2h;
     H261B_CUDA_TRY(cudaEventRecord(e->step_done[p], st));
     e->in_flight[p] = true;
     e->step_mbs[p] = total_mb;
@@ -826,13 +923,63 @@ extern "C" int h261b_session_result(h261b_engine_t *e, int32_t id, h261b_frame_r
         set_error("h261b_session_result: no completed step for session %d (wait for a step first)", id);
         return H261B_ERR_STATE;
     }
-    const Mirror &rm = e->results[best->step & 1];
+    const int p = (int)(best->step & 1);
+    const Mirror &rm = e->results[p];
     out->frame_index = best->frame;
     out->frame_type = best->type;
     out->quant = best->quant;
     out->num_mb = s->nmb;
     out->mbs = (const h261b_mb_result_t *)(rm.host + best->info_off);
-    out->levels = (const int8_t *)(rm.host + best->level_off);
+    out->levels = e->cfg.levels_to_host ? (const int8_t *)(rm.host + best->level_off) : nullptr;
+    out->bits = nullptr;
+    out->bits_bytes = 0;
+    out->bits_status = 0;
+    if (best->has_bits) {
+        const h261b_pic_info_t &pi = *(const h261b_pic_info_t *)(rm.host + best->pic_off);
+        if (pi.status != 0) {
+            out->bits_status = H261B_ERR_STATE;
+        } else if (pi.host_off >= 0) {
+            out->bits = e->bits[p].host + pi.host_off;
+            out->bits_bytes = pi.bytes;
+        } else {
+            /* the step's pictures overflowed the host arena: this one is
+             * still in the session's device slot (until the step after
+             * next); later steps get a larger arena */
+            s->bits_spill.resize((size_t)pi.bytes);
+            cudaSetDevice(e->cfg.device);
+            H261B_CUDA_TRY(cudaMemcpy(s->bits_spill.data(), s->bits_slot[p], (size_t)pi.bytes,
+                                      cudaMemcpyDeviceToHost));
+            out->bits = s->bits_spill.data();
+            out->bits_bytes = pi.bytes;
+            e->bits_want = std::max(e->bits_want, 2 * e->bits[p].cap);
+        }
+    }
+    return H261B_OK;
+}
+
+extern "C" int h261b_engine_step_bits(h261b_engine_t *e, int64_t *bytes, int32_t *pictures)
+{
+    clear_error();
+    if (!e || !bytes)
+        return H261B_ERR_ARG;
+    *bytes = 0;
+    if (pictures)
+        *pictures = 0;
+    if (e->done_step < 0)
+        return H261B_OK;
+    const int p = (int)(e->done_step & 1);
+    const Mirror &rm = e->results[p];
+    for (const Session &s : e->sessions) {
+        const Result &r = s.res[p];
+        if (!s.open || !r.has_bits || r.step != e->done_step)
+            continue;
+        const h261b_pic_info_t &pi = *(const h261b_pic_info_t *)(rm.host + r.pic_off);
+        if (pi.status == 0) {
+            *bytes += pi.bytes;
+            if (pictures)
+                (*pictures)++;
+        }
+    }
     return H261B_OK;
 }
 

@@ -42,8 +42,30 @@ typedef struct {
     int8_t cbp;
     int8_t mvx, mvy;
     int32_t cost;             /* mode-decision cost (rate control input)     */
-    int32_t reserved;
+    int32_t coef_bits;        /* bits of its blocks in the bitstream (0 when
+                                 the session writes none)                   */
 } h261b_mb_info_t;
+
+/* per-picture result of the bitstream writer (16 bytes) */
+typedef struct {
+    int32_t bytes;            /* picture size in bytes                       */
+    int32_t host_off;         /* offset in the host bitstream arena, -1 when
+                                 the arena was full (bytes stay in bits_out) */
+    int32_t status;           /* 0, or H261B_BITS_* below                    */
+    int32_t quant;            /* picture QUANT                               */
+} h261b_pic_info_t;
+
+#define H261B_BITS_BAD_RECORD  -3 /* a record the syntax cannot express      */
+#define H261B_BITS_OVERFLOW    -4 /* larger than the device slot             */
+#define H261B_BITS_MISMATCH    -5 /* a macroblock's size differs from the
+                                     encode kernel's count (an internal error) */
+
+/* step-wide state of the bitstream writer, in the descriptor arena (the
+ * descriptor upload zeroes it every step) */
+typedef struct {
+    uint32_t host_used;       /* bytes of the host arena handed out          */
+    uint32_t pad[63];
+} h261b_step_dev_t;
 
 typedef struct {
     /* pictures */
@@ -68,6 +90,11 @@ typedef struct {
     h261b_mb_info_t *info_out;    /* compact layout                         */
     int8_t *level_out;            /* [nmb][6][64], per block column-major
                                      ([u][v]); an intra DC stored as uint8   */
+    /* bitstream of the picture (QCIF / CIF sessions that write one) */
+    uint32_t *bits_out;           /* device slot, 16-byte aligned, NULL = none */
+    int32_t bits_cap;             /* bytes in bits_out                       */
+    int32_t frame_num;            /* temporal reference = frame_num & 31     */
+    h261b_pic_info_t *pic_out;
 } h261b_session_dev_t;
 
 /* phases a launch runs for each MB */
@@ -83,6 +110,14 @@ int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const uint32_t *w
                       int32_t n_work, int32_t phases, int32_t warps_per_cta, int32_t max_ctas,
                       void *stream);
 int h261b_set_quant_table(void);
+/* one CTA per session of the descriptor array that has bits_out: writes the
+ * picture into bits_out, then into the host arena (device-mapped pinned
+ * memory, host_cap bytes) at an offset drawn from step->host_used */
+int h261b_launch_bitstream(const h261b_session_dev_t *sessions_dev, int32_t n_sessions, h261b_step_dev_t *step,
+                           uint8_t *host_arena_dev, int64_t host_cap, void *stream);
+/* device slot bytes a w x h picture's bitstream may need (0: no bitstream
+ * for this size) */
+int64_t h261b_bits_slot_bytes(int32_t w, int32_t h);
 #ifdef __cplusplus
 }
 #endif

@@ -21,7 +21,9 @@ class FrameResult:
     frame_type: int
     quant: int
     mbs: np.ndarray        # RESULT_DTYPE[num_mb]
-    levels: np.ndarray     # int8 [num_mb, 6, 64], per block column-major (u * 8 + v)
+    levels: np.ndarray     # int8 [num_mb, 6, 64], per block column-major (u * 8 + v); None if not copied
+    bits: bytes = None     # the picture's H.261 bytes (sessions opened with bitstream=1)
+    bits_status: int = 0
 
     def to_abi(self, width: int) -> np.ndarray:
         """The reference's h261_macroblock_t array for this picture."""
@@ -48,21 +50,23 @@ class FrameResult:
 class Engine:
     def __init__(self, device: int = 0, max_sessions: int = 4096, hbm_budget_bytes: int = 0,
                  me_mode: int = 0, fmad: int = 1, warps_per_cta: int = 0, max_ctas: int = 0,
-                 copy_threads: int = 0):
+                 copy_threads: int = 0, levels_to_host: int = 1, bits_host_bytes: int = 0):
         lib = _lib.core()
         cfg = _lib.EngineConfig()
         lib.h261b_engine_config_default(ctypes.byref(cfg))
         cfg.device, cfg.max_sessions, cfg.hbm_budget_bytes = device, max_sessions, hbm_budget_bytes
         cfg.me_mode, cfg.fmad, cfg.warps_per_cta, cfg.max_ctas = me_mode, fmad, warps_per_cta, max_ctas
         cfg.copy_threads = copy_threads
+        cfg.levels_to_host, cfg.bits_host_bytes = levels_to_host, bits_host_bytes
         h = ctypes.c_void_p()
         check(lib.h261b_engine_create(ctypes.byref(cfg), ctypes.byref(h)), "h261b_engine_create")
         self._h = h
         self._dims = {}
 
     # -- sessions
-    def open(self, width: int, height: int, quant: int, intra_period: int = 0, denoise: int = 5) -> int:
-        c = _lib.SessionConfig(width, height, quant, intra_period, denoise)
+    def open(self, width: int, height: int, quant: int, intra_period: int = 0, denoise: int = 5,
+             bitstream: int = 0) -> int:
+        c = _lib.SessionConfig(width, height, quant, intra_period, denoise, bitstream)
         sid = ctypes.c_int32()
         check(_lib.core().h261b_session_open(self._h, ctypes.byref(c), ctypes.byref(sid)), "h261b_session_open")
         self._dims[sid.value] = (width, height)
@@ -162,10 +166,19 @@ class Engine:
         check(_lib.core().h261b_session_result(self._h, sid, ctypes.byref(r)), "h261b_session_result")
         n = r.num_mb
         mbs = np.ctypeslib.as_array((ctypes.c_uint8 * (n * 16)).from_address(r.mbs)).view(_lib.RESULT_DTYPE)
-        lv = np.ctypeslib.as_array(r.levels, shape=(n * 384,)).reshape(n, 6, 64)
+        lv = np.ctypeslib.as_array(r.levels, shape=(n * 384,)).reshape(n, 6, 64) if r.levels else None
         if copy:
-            mbs, lv = mbs.copy(), lv.copy()
-        return FrameResult(r.frame_index, r.frame_type, r.quant, mbs, lv)
+            mbs = mbs.copy()
+            lv = None if lv is None else lv.copy()
+        bits = ctypes.string_at(r.bits, r.bits_bytes) if r.bits else None
+        return FrameResult(r.frame_index, r.frame_type, r.quant, mbs, lv, bits, r.bits_status)
+
+    def step_bits(self):
+        """(bytes, pictures) of bitstream the latest completed step wrote."""
+        b, n = ctypes.c_int64(), ctypes.c_int32()
+        check(_lib.core().h261b_engine_step_bits(self._h, ctypes.byref(b), ctypes.byref(n)),
+              "h261b_engine_step_bits")
+        return b.value, n.value
 
     def recon(self, sid: int):
         w, h = self._dims[sid]

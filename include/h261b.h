@@ -61,6 +61,13 @@ typedef struct {
     int32_t copy_threads;     /* host threads copying batched submissions
                                  into the staging arena (the caller's thread
                                  included); 0 = min(8, cores / 2), 1 = none  */
+    int32_t levels_to_host;   /* 1: copy every step's quantised levels back
+                                 (h261b_frame_result_t.levels); 0: keep them
+                                 on the device (sessions that write their
+                                 bitstream on the device need no levels)    */
+    int64_t bits_host_bytes;  /* initial size of each of the two host
+                                 bitstream arenas, 0 = 8 MiB; grows when a
+                                 step's pictures do not fit                 */
 } h261b_engine_config_t;
 
 void h261b_engine_config_default(h261b_engine_config_t *cfg);
@@ -72,10 +79,16 @@ typedef struct {
     int32_t quant;            /* fixed picture QUANT 1..31                   */
     int32_t intra_period;     /* 0: only the first picture is intra          */
     int32_t denoise;          /* DCT-domain denoise strength (reference: 5)  */
+    int32_t bitstream;        /* 1: write each picture's H.261 bitstream on
+                                 the device (QCIF and CIF only), the bytes
+                                 the reference's writers produce             */
 } h261b_session_config_t;
 
-/* Device bytes one session of this size holds (pictures + state). */
+/* Device bytes one session of this size holds (pictures + state), and the
+ * bytes a session that writes its bitstream holds in addition (0 for a
+ * size the H.261 syntax has no source format for). */
 int64_t h261b_session_bytes(int32_t width, int32_t height);
+int64_t h261b_session_bits_bytes(int32_t width, int32_t height);
 
 int h261b_session_open(h261b_engine_t *e, const h261b_session_config_t *cfg, int32_t *session_id);
 int h261b_session_close(h261b_engine_t *e, int32_t session_id);
@@ -133,7 +146,8 @@ typedef struct {
     int8_t cbp;               /* bit 32>>b set when block b is coded          */
     int8_t mvx, mvy;
     int32_t cost;             /* mode-decision SATD cost                      */
-    int32_t reserved;
+    int32_t coef_bits;        /* bits of its blocks in the bitstream (TCOEFF,
+                                 intra DC, EOB); 0 without a bitstream       */
 } h261b_mb_result_t;
 
 typedef struct {
@@ -145,7 +159,14 @@ typedef struct {
     const int8_t *levels;     /* num_mb x 6 x 64 quantised levels, each
                                  block column-major (index u * 8 + v for
                                  horizontal frequency u, vertical v); an
-                                 intra DC is stored as uint8 1..255          */
+                                 intra DC is stored as uint8 1..255; NULL
+                                 when levels_to_host is 0                    */
+    const uint8_t *bits;      /* the picture's H.261 bytes (sessions with
+                                 bitstream = 1), else NULL                   */
+    int32_t bits_bytes;
+    int32_t bits_status;      /* 0, or negative: the picture has no
+                                 bitstream (H261B_ERR_STATE: a record the
+                                 syntax cannot express)                      */
 } h261b_frame_result_t;
 
 /* Results of the latest completed step that encoded this session (pointers
@@ -160,6 +181,10 @@ int h261b_session_result(h261b_engine_t *e, int32_t session_id, h261b_frame_resu
 int h261b_engine_step_records(h261b_engine_t *e, const h261b_mb_result_t **records, int64_t *count,
                               int64_t *step);
 
+/* Bitstream bytes and pictures the latest completed step wrote, over its
+ * open sessions that write one. */
+int h261b_engine_step_bits(h261b_engine_t *e, int64_t *bytes, int32_t *pictures);
+
 /* Copy the session's latest reconstruction (packed planes) to the host. */
 int h261b_session_recon(h261b_engine_t *e, int32_t session_id, uint8_t *y, uint8_t *cb, uint8_t *cr);
 
@@ -170,7 +195,9 @@ int h261b_result_to_abi(const h261b_frame_result_t *r, int32_t width, h261_macro
 /* Device time of the last step's kernel in milliseconds (CUDA events). */
 int h261b_engine_last_kernel_ms(h261b_engine_t *e, float *ms);
 /* Bytes the last step copied host->device (descriptors, work list,
- * pictures) and device->host (records and levels). */
+ * pictures) and device->host (records, picture records, levels when copied;
+ * the bitstream bytes, which the device writes into mapped host memory,
+ * are h261b_engine_step_bits()). */
 int h261b_engine_last_copy_bytes(h261b_engine_t *e, int64_t *h2d, int64_t *d2h);
 /* Throughput of the 4-pixel SAD primitive the motion search uses, measured
  * on the device with every SM busy: absolute differences per second. */

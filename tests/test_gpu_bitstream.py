@@ -1,0 +1,118 @@
+"""The device bitstream writer: every picture's H.261 bytes must be the
+reference's.  Pinned against the golden fixtures (per-picture SHA-256 of the
+bitstream the reference produced on a B200) and against the oracle's
+restatement of the reference writers on the engine's own records."""
+import glob
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import oracle as O
+from h261enc_cuda_b200 import synth
+from h261enc_cuda_b200.engine import Engine
+
+HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+sys.path.insert(0, HERE)
+import make_golden as MG  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+FIXTURES = sorted(glob.glob(os.path.join(HERE, "*.json")))
+IDS = [os.path.basename(p)[:-5] for p in FIXTURES]
+
+
+@pytest.mark.parametrize("levels_to_host", [1, 0])
+@pytest.mark.parametrize("path", FIXTURES, ids=IDS)
+def test_bitstream_matches_reference_fixture(gpu, path, levels_to_host):
+    """Fixed-QUANT cases as they are; the rate-controlled case with the
+    QUANT sequence the reference's rate control chose."""
+    g = json.load(open(path))
+    opt = g["options"]
+    fr = MG.make_input(g["case"])
+    w, h = g["width"], g["height"]
+    with Engine(warps_per_cta=4, levels_to_host=levels_to_host) as e:
+        sid = e.open(w, h, max(opt.get("quant", 0), 1), intra_period=opt.get("intra", 0), bitstream=1)
+        stream = b""
+        for i, want in enumerate(g["per_frame"]):
+            e.submit_frame(sid, fr[i], quant=want["quant"])
+            e.step()
+            e.sync()
+            r = e.result(sid)
+            assert r.bits_status == 0
+            assert (r.levels is None) == (levels_to_host == 0)
+            assert len(r.bits) == want["bytes"], f"picture {i}: {len(r.bits)} != {want['bytes']} bytes"
+            assert MG.sha(r.bits) == want["bits"], f"picture {i}: bitstream differs"
+            stream += r.bits
+    assert MG.sha(stream) == g["stream_sha256"]
+
+
+@pytest.mark.parametrize("preset,w,h,quant", [(0, 176, 144, 1), (1, 352, 288, 2), (3, 176, 144, 5),
+                                              (2, 352, 288, 17), (0, 176, 144, 31)])
+def test_bitstream_matches_oracle_writer(gpu, preset, w, h, quant):
+    fr = synth.clip(preset, w, h, 50 + quant, 5)
+    with Engine(warps_per_cta=4) as e:
+        sid = e.open(w, h, quant, intra_period=3, bitstream=1)
+        for i in range(fr.shape[0]):
+            e.submit_frame(sid, fr[i])
+            e.step()
+            e.sync()
+            r = e.result(sid)
+            want = O.write_picture_oracle(r.to_abi(w), w, h, i, r.frame_type, quant)
+            assert r.bits == want, f"picture {i}: {len(r.bits)} vs {len(want)} bytes"
+            # the per-MB coefficient counts add up to the picture
+            assert int(r.mbs["coef_bits"].sum()) < 8 * len(r.bits)
+
+
+def test_bitstream_batch_pipelined_matches_oracle_stream(gpu):
+    """Mixed sessions, steps issued back to back, results read one step late."""
+    specs = [(176, 144, 8, 31), (352, 288, 12, 32), (176, 144, 3, 33), (352, 288, 24, 34), (176, 144, 16, 35)]
+    n = 6
+    clips = [synth.clip(2, w, h, seed, n) for (w, h, q, seed) in specs]
+    want = [O.encode_stream(c, w, h, quant=q)[0] for c, (w, h, q, _) in zip(clips, specs)]
+    got = [b"" for _ in specs]
+    with Engine(warps_per_cta=4, levels_to_host=0) as e:
+        sids = [e.open(w, h, q, bitstream=1) for (w, h, q, _) in specs]
+        for i in range(n + 1):
+            if i < n:
+                e.submit_frames(sids, [c[i] for c in clips])
+                e.step()
+            if i > 0:
+                e.wait_previous() if i < n else e.sync()
+                total = 0
+                for k, sid in enumerate(sids):
+                    r = e.result(sid)
+                    assert r.frame_index == i - 1
+                    got[k] += r.bits
+                    total += len(r.bits)
+                assert e.step_bits() == (total, len(sids))
+    for k in range(len(specs)):
+        assert got[k] == want[k], f"session {k}"
+
+
+def test_bitstream_host_arena_overflow_falls_back(gpu):
+    """A host arena too small for a step: the pictures that miss it are read
+    from the device slots, later steps get a larger arena."""
+    fr = synth.clip(1, 352, 288, 7, 4)
+    want = O.encode_stream(fr, 352, 288, quant=2)[1]
+    with Engine(warps_per_cta=4, bits_host_bytes=4096) as e:
+        a = e.open(352, 288, 2, bitstream=1)
+        b = e.open(352, 288, 2, bitstream=1)
+        for i in range(fr.shape[0]):
+            e.submit_frames([a, b], [fr[i], fr[i]])
+            e.step()
+            e.sync()
+            ra, rb = e.result(a), e.result(b)
+            assert len(ra.bits) == want[i] and ra.bits == rb.bits
+
+
+def test_bitstream_refused_for_other_sizes(gpu):
+    with Engine(warps_per_cta=4) as e:
+        with pytest.raises(RuntimeError):
+            e.open(320, 240, 8, bitstream=1)
+        sid = e.open(320, 240, 8)          # the core itself takes any multiple of 16
+        e.submit_frame(sid, synth.clip(0, 320, 240, 1, 1)[0])
+        e.step()
+        e.sync()
+        assert e.result(sid).bits is None
