@@ -1,32 +1,33 @@
 #!/usr/bin/env python
-"""Encoded macroblocks per second of the B200 H.261 core.
+"""Encoded macroblocks per second of the B200 H.261 encoder.
 
 One step = one frame-step of the workload: the next picture of every stream
 of the batch, encoded in one launch of the core (motion search, mode
 decision, motion compensation with the loop filter, DCT, denoise,
-quantisation, dequantisation, IDCT, reconstruction).  Workload: ``batch64``
-(40 QCIF + 24 CIF streams, QUANT 4..24, seeded synthetic content; see
-h261enc_cuda_b200/workloads.py).
+quantisation, dequantisation, IDCT, reconstruction) followed by one launch
+of the bitstream writer (every picture's H.261 bytes).  Workload:
+``batch64`` (40 QCIF + 24 CIF streams, QUANT 4..24, lengths 30..300,
+seeded synthetic content; see h261enc_cuda_b200/workloads.py).
 
   value   device throughput: pictures already in HBM, L2 flushed (256 MiB
-          write) before every timed step, the step kernel timed with CUDA
+          write) before every timed step, both kernels timed with CUDA
           events on the engine's stream;
   e2e     the same through the public API with host buffers: every step
           copies the pictures of all streams from host memory into the
           pinned staging arena (h261b_engine_submit_batch, the engine's copy
-          threads), moves them to the device, encodes, and copies records
-          and levels back; the host reads step k-1's records while step k
-          runs (two streams);
+          threads), moves them to the device, encodes, writes the
+          bitstreams into mapped host memory and copies the MB records
+          back; the host moves step k-1's bitstreams out while step k runs;
   single_stream  the same streams one at a time (one picture per step,
           synchronous), the plain single-stream path;
   latency_ms     per-picture latency: batched = submit of a step -> its
-          records read on the host (pipelined), single = one synchronous
+          bitstreams on the host (pipelined), single = one synchronous
           picture.
 
-``--impl reference`` times the CPU restatement of the reference's device
-path (oracle/) on all host cores instead.  Under torchrun every rank encodes
-its own batch (weak scaling, no collective on the data path); rank 0 prints
-one JSON line.
+``--impl reference`` times the CPU restatement of the reference's encoder
+(oracle/: device path, frame loop, bitstream writer) on all host cores
+instead.  Under torchrun every rank encodes its own batch (weak scaling, no
+collective on the data path); rank 0 prints one JSON line.
 """
 from __future__ import annotations
 
@@ -172,8 +173,9 @@ def dist_setup(args):
 # ------------------------------------------------------------ CPU baseline
 
 def cpu_baseline(streams, frames_per_stream: int, threads: int):
-    """The oracle (C restatement of the reference's device path) over a
-    bounded sample: each task encodes one stream's first pictures."""
+    """The oracle (C restatement of the reference's encoder: device path,
+    rate-control-free frame loop and bitstream writer) over a bounded
+    sample: each task encodes one stream's first pictures to H.261 bytes."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     from h261enc_cuda_b200 import workloads
@@ -181,7 +183,7 @@ def cpu_baseline(streams, frames_per_stream: int, threads: int):
 
     def task(i):
         s = streams[i]
-        O.encode_sequence(clips[i], s.width, s.height, s.quant)
+        O.encode_stream(clips[i], s.width, s.height, quant=s.quant)
         return s.num_mb * frames_per_stream
 
     O.lib()
@@ -207,7 +209,7 @@ def reference_arm(args, world, rank):
         times.append(el)
         total += mbs
     value = total / sum(times)
-    sample = f"{len(streams)} streams x {frames} pictures per step (oracle, C, -O2)"
+    sample = f"{len(streams)} streams x {frames} pictures to bitstreams per step (oracle, C, -O2)"
     line = {"impl": "reference", "metric": "encoded MB/s", "value": value, "unit": "MB/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
@@ -244,14 +246,16 @@ def device_clips(streams, clip_len, device):
 
 class Runner:
     """Keeps the workload's slots full: a stream that reaches its length is
-    closed and a new session (same geometry and QUANT) takes the slot.  The
-    engine returns a closed session's device slot to its pool once the
-    steps in flight that use it have completed, so nothing drains here."""
+    replaced by a new session (same geometry and QUANT) and closed once its
+    last picture has been read (``retire``).  The engine returns a closed
+    session's device slot to its pool when the steps in flight that use it
+    have completed, so nothing drains here."""
 
     def __init__(self, engine, streams, pools):
         self.e, self.streams, self.pools = engine, streams, pools
-        self.sids = [engine.open(s.width, s.height, s.quant) for s in streams]
+        self.sids = [engine.open(s.width, s.height, s.quant, bitstream=1) for s in streams]
         self.pos = [0] * len(streams)
+        self.ending = []
         # host pictures: one contiguous (clip, W*H*3/2) array per stream
         self.base = np.array([p[1].ctypes.data for p in pools], np.uint64)
         self.fbytes = np.array([p[1].shape[1] for p in pools], np.uint64)
@@ -262,12 +266,18 @@ class Runner:
         idx = np.empty(len(self.streams), np.uint64)
         for k, s in enumerate(self.streams):
             if self.pos[k] >= s.length:
-                self.e.close(self.sids[k])
-                self.sids[k] = self.e.open(s.width, s.height, s.quant)
+                self.ending.append(self.sids[k])
+                self.sids[k] = self.e.open(s.width, s.height, s.quant, bitstream=1)
                 self.pos[k] = 0
             idx[k] = workloads.clip_index(self.pos[k], CLIP_LEN)
             self.pos[k] += 1
         return idx
+
+    def retire(self):
+        """Close the streams whose last picture was in the step just read."""
+        for sid in self.ending:
+            self.e.close(sid)
+        self.ending = []
 
     def queue_device(self):
         idx = self._advance()
@@ -293,19 +303,23 @@ def ours(args, world, rank, local, dist):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     peak_sad = sad_peak(local)
 
-    eng = Engine(device=local, max_sessions=4 * len(streams))
+    # every stream writes its H.261 bitstream on the device; the levels stay
+    # in HBM (the bitstream is the output)
+    eng = Engine(device=local, max_sessions=4 * len(streams), levels_to_host=0)
     run = Runner(eng, streams, pools)
     # warm-up (includes the launch-shape tuning steps), both input paths
     for i in range(max(args.warmup, 8)):
         run.queue_device() if i % 2 else run.queue_host()
         eng.step()
         eng.sync()
+        run.retire()
 
-    # ---- value: device-resident pictures, L2 flushed, kernel events
+    # ---- value: device-resident pictures, L2 flushed, the step's two
+    # kernels (encode, bitstream) timed with CUDA events on its stream
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    kernel_ms = []
+    kernel_ms, bits_ms, bits_bytes = [], [], []
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             flush.zero_()
@@ -313,21 +327,33 @@ def ours(args, world, rank, local, dist):
             run.queue_device()
             eng.step()
             kernel_ms.append(eng.last_kernel_ms())
-        eng.sync()
+            bits_ms.append(eng.last_bits_ms())
+            eng.sync()
+            bits_bytes.append(eng.step_bits()[0])
+            run.retire()
     torch.cuda.synchronize()
-    total_ms = float(sum(kernel_ms))
+    total_ms = float(sum(kernel_ms) + sum(bits_ms))
     if dist:
         t = torch.tensor([total_ms], device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     value = mb_per_step * args.steps * world / (total_ms * 1e-3)
 
-    # ---- e2e: host pictures through the public API, results read back.
-    # Step k is issued, then the host waits for step k-1 and reads its MB
-    # records while step k runs (the engine alternates two streams).
-    chk = np.uint64(0)
+    # ---- e2e: host pictures in, bitstreams out, through the public API.
+    # Step k is issued, then the host waits for step k-1 and moves its
+    # pictures' bytes out of the host arena while step k runs (the engine
+    # alternates two streams).
+    out = np.empty(64 << 20, np.uint8)
     lat, issued = [], []
     h2d = d2h = 0
+
+    def consume():
+        nonlocal d2h
+        pics, span = eng.step_pictures()
+        assert pics.size == len(streams) and (pics["status"] == 0).all()
+        out[:span.size] = span
+        d2h += int(pics["bytes"].sum())
+
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -340,12 +366,12 @@ def ours(args, world, rank, local, dist):
         h2d, d2h = h2d + b_in, d2h + b_out
         if it > 0:
             eng.wait_previous()
-            _, recs = eng.step_records()
-            chk ^= np.bitwise_xor.reduce(recs.view(np.uint64))
+            consume()
+            run.retire()
             lat.append((time.perf_counter() - issued[it - 1]) * 1e3)
     eng.sync()
-    _, recs = eng.step_records()
-    chk ^= np.bitwise_xor.reduce(recs.view(np.uint64))
+    consume()
+    run.retire()
     lat.append((time.perf_counter() - issued[-1]) * 1e3)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
@@ -360,17 +386,17 @@ def ours(args, world, rank, local, dist):
 
     # ---- single stream: the same streams one at a time, one picture per step
     single_lat, single_mbs = [], 0
-    eng1 = Engine(device=local, max_sessions=8, warps_per_cta=4)
+    eng1 = Engine(device=local, max_sessions=8, warps_per_cta=4, levels_to_host=0)
     per_stream = 3
     t0 = time.perf_counter()
     for k, s in enumerate(streams):
-        sid = eng1.open(s.width, s.height, s.quant)
+        sid = eng1.open(s.width, s.height, s.quant, bitstream=1)
         for i in range(per_stream):
             ts = time.perf_counter()
             eng1.submit_frame(sid, pools[k][1][i])
             eng1.step()
             eng1.sync()
-            eng1.result(sid, copy=False)
+            assert eng1.result(sid, copy=False).bits
             single_lat.append((time.perf_counter() - ts) * 1e3)
             single_mbs += s.num_mb
         eng1.close(sid)
@@ -385,39 +411,42 @@ def ours(args, world, rank, local, dist):
         return
 
     peak, peak_kind = hbm_peak()
+    mean_kernel = float(np.mean(kernel_ms))
     mean_ms = total_ms / args.steps
-    achieved = mb_per_step * ALG_BYTES_PER_MB / (mean_ms * 1e-3) / 1e9
+    achieved = mb_per_step * ALG_BYTES_PER_MB / (mean_kernel * 1e-3) / 1e9
     tr = ncu_traffic_per_mb()
-    sad_rate = mb_per_step * SAD_PER_MB / (mean_ms * 1e-3)
+    sad_rate = mb_per_step * SAD_PER_MB / (mean_kernel * 1e-3)
     line = {
-        "metric": "encoded MB/s (batched 64 mixed QCIF/CIF streams, bit-exact to the reference)",
+        "metric": "encoded MB/s (batched 64 mixed QCIF/CIF streams to H.261 bitstreams, bit-exact to the reference)",
         "value": value, "unit": "MB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": mean_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u8", "data": "synthetic (seeded pan/object clips, 24-picture ping-pong per stream)",
         "config": {"workload": args.workload, "streams": len(streams), "mb_per_step": mb_per_step,
                    "me_mode": "reference (11x11 grid + 7x7 refinement)",
                    "l2": "flushed before every timed step (256 MiB write)", "parallelism": f"sessions x{world}"},
+        "kernels_ms": {"encode": mean_kernel, "bitstream": float(np.mean(bits_ms))},
+        "bitstream_bytes_per_step": float(np.mean(bits_bytes)),
         "e2e": {"value": e2e, "unit": "MB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "host_input": "pageable numpy clips -> pinned arena -> HBM, every step",
+                "path": "host pictures (pageable) -> pinned arena -> HBM; records + H.261 bitstreams back",
                 "l2": "not flushed (steady pipeline: inputs arrive from the host each step)"},
         "single_stream": {"value": single, "unit": "MB/s", "pictures": len(single_lat)},
         "batch_vs_single": value / single,
         "latency_ms": {"batched_p50": float(np.percentile(lat, 50)), "batched_p99": float(np.percentile(lat, 99)),
                        "single_p50": float(np.percentile(single_lat, 50)),
                        "single_p99": float(np.percentile(single_lat, 99))},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_source": peak_kind,
+        "roofline": {"bound": "hbm", "kernel": "step_kernel (encode)", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": (tr * mb_per_step) if tr else None},
         "sad_roofline": {"achieved": sad_rate, "peak": peak_sad, "unit": "absdiff/s", "frac": sad_rate / peak_sad,
                          "peak_source": "project microbenchmark of the search's SAD step"},
-        "gpu_launches": args.steps,
+        "gpu_launches": 2 * args.steps,
         "clocks": clk.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         mbs, el = cpu_baseline(streams, 3, threads)
         line["cpu_baseline"] = {"value": mbs / el, "unit": "MB/s", "cores": threads, "kind": "port",
-                                "sample": f"{len(streams)} streams x 3 pictures (oracle, C)"}
+                                "sample": f"{len(streams)} streams x 3 pictures to bitstreams (oracle, C)"}
     print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -52,6 +52,8 @@ MD_DTYPE = np.dtype([("cost", "<i4"), ("qadj", "<i4"), ("type", "<i4"), ("flags"
 MB_DTYPE = np.dtype([("addr", "<i4"), ("type", "<i4"), ("flags", "<i4"), ("quant", "<i4"),
                      ("mv", "<i4", 2), ("cbp", "<i4"), ("tcoeff", "<i4", (6, 64)),
                      ("mb_x", "<i4"), ("mb_y", "<i4")])
+PICTURE_DTYPE = np.dtype([("session_id", "<i4"), ("frame_index", "<i4"), ("bytes", "<i4"), ("status", "<i4"),
+                          ("bits", "<u8")])
 RESULT_DTYPE = np.dtype([("type", "<i2"), ("flags", "<i2"), ("quant", "i1"), ("cbp", "i1"),
                          ("mvx", "i1"), ("mvy", "i1"), ("cost", "<i4"), ("coef_bits", "<i4")])
 assert ME_MB_DTYPE.itemsize == 20 and MD_DTYPE.itemsize == 24 and MB_DTYPE.itemsize == 1572
@@ -117,6 +119,9 @@ def core() -> ctypes.CDLL:
                                             POINTER(POINTER(c_uint8)), POINTER(POINTER(c_uint8))]
         lib.h261b_engine_submit_batch.argtypes = [c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
                                                   c_void_p]
+        lib.h261b_engine_last_bits_ms.argtypes = [c_void_p, POINTER(c_float)]
+        lib.h261b_engine_step_pictures.argtypes = [c_void_p, c_int32, c_void_p, POINTER(c_int32),
+                                                   POINTER(c_void_p), POINTER(ctypes.c_int64)]
         lib.h261b_engine_step_bits.argtypes = [c_void_p, POINTER(ctypes.c_int64), POINTER(c_int32)]
         lib.h261b_session_bits_bytes.argtypes = [c_int32, c_int32]
         lib.h261b_session_bits_bytes.restype = c_int64

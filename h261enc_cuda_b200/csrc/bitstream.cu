@@ -7,26 +7,34 @@
  * QCIF / CIF order, macroblocks with MBA, MTYPE, MQUANT, MVD, CBP, TCOEFF
  * and EOB, the last byte zero-padded (src/h261_bitstream.c:64-76).
  *
- * One CTA per picture:
- *   A  every GOB is one warp, one lane per macroblock (the 33rd by all
- *      lanes): the address increment, quantiser in force and vector
- *      predictor of a macroblock depend only on earlier records of its GOB,
- *      so ballots over the GOB's coded / COEFF / MC flags give them all at
- *      once.  Header bits plus the coefficient bits the encode kernel
- *      counted (h261b_mb_info_t.coef_bits) give every macroblock's size; a
- *      warp scan gives its offset in the GOB.
- *   B  one thread scans the GOB sizes; the picture's words are cleared.
- *   C  warps take macroblocks: each assembles its macroblock in a shared
- *      staging buffer (lane 0 the header; eight lanes per block, each lane
- *      eight consecutive coefficients of the transmission order, a scan for
- *      the code offsets) and stores it; only a macroblock's first and last
- *      word can be shared with a neighbour and are ORed in with atomics.
- *   D  the picture is copied to the host arena (mapped pinned memory) at an
- *      offset drawn with one atomic, so no separate copy is issued for it.
+ * Four launches; the macroblock-parallel ones take contiguous ranges of the
+ * step's work list, one warp per macroblock, so that every SM takes part
+ * whatever the mix of picture sizes, and kernel boundaries order the
+ * phases (nothing waits on a flag):
+ *
+ *   codes   the macroblock's coded blocks, four at a time with eight lanes
+ *           per block (lane j holds positions 8j..8j+7 of the transmission
+ *           order): runs from the block's nonzero mask, TCOEFF / escape /
+ *           DC / EOB codes, a scan for their offsets, assembled in shared
+ *           memory and stored as the MB's coefficient bit string.
+ *   layout  one CTA per picture, a warp per GOB with a lane per macroblock:
+ *           the address increments, quantiser in force and vector
+ *           predictors come from ballots over the GOB's coded / COEFF / MC
+ *           flags; MB sizes, a scan over the GOB and one over the GOBs give
+ *           every macroblock's position; the picture is cleared and gets its
+ *           picture and GOB headers.
+ *   pack    every coded macroblock writes its header and shifts its bit
+ *           string into place; a macroblock's first and last word can be
+ *           shared with its neighbours and are ORed in with atomics.
+ *   copy    one CTA per picture copies it into the host arena (mapped
+ *           pinned memory) at an offset drawn with one atomic.
  */
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdint.h>
+
+#include <algorithm>
+#include <cstring>
 
 #include "h261b_device.h"
 #include "vlc_tables.h"
@@ -35,45 +43,68 @@ namespace h261b {
 namespace {
 
 constexpr unsigned FULL = 0xFFFFFFFFu;
-constexpr int BS_WARPS = 8;
-constexpr int BS_THREADS = BS_WARPS * 32;
-constexpr int MAX_MB = 396;          /* CIF */
-/* one macroblock: header <= 57 bits, six blocks <= 6 * (8 + 63 * 20 + 2);
- * plus up to 31 bits of offset into the first word */
-constexpr int MB_MAX_BITS = 57 + 6 * (64 * 20 + 2);
-constexpr int STAGE_WORDS = (MB_MAX_BITS + 31 + 31) / 32 + 1;
+constexpr int VLC_WARPS = 8;
+constexpr int VLC_THREADS = VLC_WARPS * 32;
+constexpr int MB_WORDS = H261B_VLC_MB_WORDS;
+/* header bits of one macroblock at most: MBA 11, MTYPE 10, MQUANT 5,
+ * MVD 2 x 11, CBP 9 */
+constexpr int MB_HDR_MAX = 57;
 
-struct BsSmem {
-    /* vector-accessed arrays first, on 16-byte boundaries */
-    alignas(16) int8_t blk[BS_WARPS][4][64];   /* column-major levels of the blocks in flight */
-    alignas(16) uint32_t stage[BS_WARPS][STAGE_WORDS];
+struct CodesSmem {
+    alignas(16) int8_t blk[VLC_WARPS][4][64];   /* column-major levels of the blocks in flight */
+    alignas(16) uint32_t stage[VLC_WARPS][MB_WORDS];
     uint16_t tc[27][16];
-    uint8_t zz_cm[64];               /* column-major index of the k-th coefficient sent */
-    int32_t mb_off[MAX_MB];          /* bit offset of the MB within its GOB */
-    int32_t mb_len[MAX_MB];          /* its size in bits, 0 = not coded */
-    uint32_t mb_plan[MAX_MB];        /* header fields, see plan_* */
-    int32_t gob_bits[12];
-    int32_t gob_off[12];
-    int32_t total_bits;
-    int32_t status;
-    int32_t host_off;
+    uint8_t zz_cm[64];                           /* column-major index of the k-th coefficient sent */
 };
-static_assert(offsetof(BsSmem, blk) % 16 == 0 && offsetof(BsSmem, stage) % 16 == 0, "vector alignment");
 
-/* header plan of a macroblock: address increment, MTYPE, MQUANT flag and
- * the two wrapped vector differences */
-__device__ __forceinline__ uint32_t plan_pack(int addr, int mtype, int mq, int dx, int dy)
+__device__ __forceinline__ uint32_t bswap(uint32_t x) { return __byte_perm(x, 0, 0x0123); }
+
+/* OR a code of len <= 32 bits into MSB-first words at bit position pos of
+ * a buffer of `words` words; a position outside it is not written and
+ * counts as an error */
+__device__ __forceinline__ void put_bits(uint32_t *w, int words, int pos, uint32_t code, int len, int &oob)
 {
-    return (uint32_t)addr | ((uint32_t)mtype << 6) | ((uint32_t)mq << 10) | ((uint32_t)(dx + 16) << 11) |
-           ((uint32_t)(dy + 16) << 16);
+    if (len <= 0)
+        return;
+    if (pos < 0 || pos + len > words * 32) {
+        oob = 1;
+        return;
+    }
+    const int word = pos >> 5, end = (pos & 31) + len;
+    if (end <= 32) {
+        atomicOr(&w[word], code << (32 - end));
+    } else {
+        atomicOr(&w[word], code >> (end - 32));
+        atomicOr(&w[word + 1], code << (64 - end));
+    }
+}
+
+/* the same on a picture in device memory, whose words hold the stream's
+ * bytes in order (byte-swapped) */
+__device__ __forceinline__ void put_bits_pic(uint32_t *w, int64_t words, int64_t pos, uint32_t code, int len,
+                                             int &oob)
+{
+    if (len <= 0)
+        return;
+    if (pos < 0 || pos + len > words * 32) {
+        oob = 1;
+        return;
+    }
+    const int64_t word = pos >> 5;
+    const int end = (int)(pos & 31) + len;
+    if (end <= 32) {
+        atomicOr(&w[word], bswap(code << (32 - end)));
+    } else {
+        atomicOr(&w[word], bswap(code >> (end - 32)));
+        atomicOr(&w[word + 1], bswap(code << (64 - end)));
+    }
 }
 
 __device__ __forceinline__ int wrap_mvd(int d) { return ((d + 16) & 31) - 16; }
 
 __device__ __forceinline__ void mvd_code(int w, uint32_t &code, int &len)
 {
-    const int a = w < 0 ? -w : w;
-    const uint16_t e = c_vlc_mvd[a];
+    const uint16_t e = c_vlc_mvd[w < 0 ? -w : w];
     len = e >> 8;
     code = (uint32_t)(e & 0xFF) - (w > 0 ? 1u : 0u);
 }
@@ -94,251 +125,102 @@ __device__ __forceinline__ int mtype_of(int type, int flags, int mq)
     }
 }
 
-/* OR a code of len <= 32 bits into the MSB-first staging words at bit
- * position pos; a position outside the buffer is not written and counts
- * as an error */
-__device__ __forceinline__ void put_bits(uint32_t *w, int pos, uint32_t code, int len, int &oob)
+/* header plan: address increment, MTYPE, MQUANT flag, wrapped MVDs */
+__device__ __forceinline__ uint32_t plan_pack(int addr, int mtype, int mq, int dx, int dy)
 {
-    if (len <= 0)
-        return;
-    if (pos < 0 || pos + len > STAGE_WORDS * 32) {
-        oob = 1;
-        return;
-    }
-    const int word = pos >> 5, off = pos & 31;
-    const int end = off + len;
-    if (end <= 32) {
-        atomicOr(&w[word], code << (32 - end));
-    } else {
-        atomicOr(&w[word], code >> (end - 32));
-        atomicOr(&w[word + 1], code << (64 - end));
-    }
+    return (uint32_t)addr | ((uint32_t)mtype << 6) | ((uint32_t)mq << 10) | ((uint32_t)(dx + 16) << 11) |
+           ((uint32_t)(dy + 16) << 16);
 }
 
-__device__ __forceinline__ uint32_t bswap(uint32_t x) { return __byte_perm(x, 0, 0x0123); }
-
-/* same, on the picture's words in device memory (stored byte-swapped, so
- * that their bytes are the stream's bytes) */
-__device__ __forceinline__ void put_bits_global(uint32_t *w, int64_t pos, uint32_t code, int len)
+/* coded blocks of a record: all six of an intra MB, the CBP of an inter MB
+ * with COEFF, else none; bit (5 - b) = block b */
+__device__ __forceinline__ int coded_blocks(const h261b_mb_info_t &r)
 {
-    const int64_t word = pos >> 5;
-    const int off = (int)(pos & 31), end = off + len;
-    if (end <= 32) {
-        atomicOr(&w[word], bswap(code << (32 - end)));
-    } else {
-        atomicOr(&w[word], bswap(code >> (end - 32)));
-        atomicOr(&w[word + 1], bswap(code << (64 - end)));
-    }
+    if (r.type == H261B_MB_TYPE_INTRA)
+        return 63;
+    return (r.flags & H261B_MB_COEFF) ? (r.cbp & 63) : 0;
 }
 
-__global__ void __launch_bounds__(BS_THREADS) bitstream_kernel(const h261b_session_dev_t *sessions,
-                                                               h261b_step_dev_t *step, uint8_t *host_arena,
-                                                               int64_t host_cap)
+/* header of one macroblock from its record and its GOB neighbours' state:
+ * plan and size in bits; bad when the syntax has no code for it */
+struct MbHeader {
+    uint32_t plan;
+    int bits;
+    bool bad;
+};
+
+__device__ __forceinline__ MbHeader mb_header(const h261b_mb_info_t &r, int addr, int q_state, bool mv_ok, int pmx,
+                                              int pmy)
 {
-    const h261b_session_dev_t &S = sessions[blockIdx.x];
-    if (!S.bits_out)
-        return;
-    __shared__ BsSmem sm;
+    const bool intra = r.type == H261B_MB_TYPE_INTRA;
+    const int mq = intra ? (r.quant != q_state) : (r.quant != q_state && (r.flags & H261B_MB_COEFF));
+    const int mt = mtype_of(r.type, r.flags, mq);
+    const int dx = wrap_mvd(r.mvx - (mv_ok ? pmx : 0)), dy = wrap_mvd(r.mvy - (mv_ok ? pmy : 0));
+    int h = (c_vlc_mba[addr] >> 8) + (mt >= 0 ? c_vlc_mtype_len[mt] : 0) + (mq ? 5 : 0);
+    if (!intra && (r.flags & H261B_MB_MC))
+        h += (c_vlc_mvd[dx < 0 ? -dx : dx] >> 8) + (c_vlc_mvd[dy < 0 ? -dy : dy] >> 8);
+    const int cbp = coded_blocks(r);
+    if (!intra && cbp)
+        h += c_vlc_cbp[cbp] >> 8;
+    MbHeader o;
+    o.plan = plan_pack(addr, mt < 0 ? 0 : mt, mq, dx, dy);
+    o.bits = h;
+    o.bad = mt < 0 || (!intra && (r.flags & H261B_MB_COEFF) && cbp == 0);
+    return o;
+}
+
+/* the range of the work list a warp takes: contiguous, so that its
+ * macroblocks mostly share a picture */
+__device__ __forceinline__ void warp_range(int32_t n_work, int &lo, int &hi)
+{
+    const int nwarps = gridDim.x * VLC_WARPS;
+    const int w = blockIdx.x * VLC_WARPS + (threadIdx.x >> 5);
+    const int chunk = (n_work + nwarps - 1) / nwarps;
+    lo = min(w * chunk, n_work);
+    hi = min(lo + chunk, n_work);
+}
+
+/* ---- codes: each macroblock's coefficient bit string */
+__global__ void __launch_bounds__(VLC_THREADS) codes_kernel(const h261b_session_dev_t *sessions,
+                                                            const uint32_t *work, int32_t n_work)
+{
+    __shared__ CodesSmem sm;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const bool cif = S.mbw == 22;
-    const int ngob = cif ? 12 : 3, nmb = S.mbw * S.mbh;
-    const int gq = S.quant;
-    const h261b_mb_info_t *info = S.info_out;
-
-    for (int i = tid; i < 27 * 16; i += BS_THREADS)
+    for (int i = tid; i < 27 * 16; i += VLC_THREADS)
         (&sm.tc[0][0])[i] = (&c_vlc_tcoeff[0][0])[i];
     if (tid < 64) {
-        /* column-major index of zig-zag position tid */
         for (int v = 0; v < 8; v++)
             for (int u = 0; u < 8; u++)
                 if (zigzag_index(v, u) == tid)
                     sm.zz_cm[tid] = (uint8_t)(u * 8 + v);
     }
-    if (tid == 0)
-        sm.status = 0;
-    __syncthreads();
-
-    /* ---- A: macroblock headers and sizes, one warp per GOB */
-    for (int g = warp; g < ngob; g += BS_WARPS) {
-        const int x0 = cif ? (g & 1) * 11 : 0, y0 = (cif ? g >> 1 : g) * 3;
-        const int mi = (y0 + lane / 11) * S.mbw + x0 + lane % 11;
-        const int m32 = (y0 + 2) * S.mbw + x0 + 10;
-        const h261b_mb_info_t r = info[mi];
-        const h261b_mb_info_t r32 = info[m32];
-        const uint32_t C = __ballot_sync(FULL, r.flags != 0);
-        const uint32_t K = __ballot_sync(FULL, (r.flags & H261B_MB_COEFF) != 0);
-        const uint32_t M = __ballot_sync(FULL, (r.flags & H261B_MB_MC) != 0);
-        const int prev_mvx = __shfl_up_sync(FULL, (int)r.mvx, 1), prev_mvy = __shfl_up_sync(FULL, (int)r.mvy, 1);
-        const uint32_t below = (1u << lane) - 1u;
-        /* quantiser in force: the last COEFF macroblock before, else GQUANT */
-        const uint32_t kb = K & below;
-        const int qv = __shfl_sync(FULL, (int)r.quant, kb ? 31 - __clz((int)kb) : lane);
-        const int qv32 = __shfl_sync(FULL, (int)r.quant, K ? 31 - __clz((int)K) : 0);
-        const int mvx31 = __shfl_sync(FULL, (int)r.mvx, 31), mvy31 = __shfl_sync(FULL, (int)r.mvy, 31);
-
-        int bits = 0, bits32 = 0, bad = 0;
-        /* lane's macroblock */
-        if (r.flags != 0) {
-            const uint32_t cb = C & below;
-            const int addr = cb ? lane - (31 - __clz((int)cb)) : lane + 1;
-            const int qs = kb ? qv : gq;
-            const bool intra = r.type == H261B_MB_TYPE_INTRA;
-            const int mq = intra ? (r.quant != qs) : (r.quant != qs && (r.flags & H261B_MB_COEFF));
-            const int mt = mtype_of(r.type, r.flags, mq);
-            const bool ok = lane > 0 && lane % 11 != 0 && ((M >> (lane - 1)) & 1u);
-            const int dx = wrap_mvd(r.mvx - (ok ? prev_mvx : 0)), dy = wrap_mvd(r.mvy - (ok ? prev_mvy : 0));
-            int h = (c_vlc_mba[addr] >> 8) + (mt >= 0 ? c_vlc_mtype_len[mt] : 0) + (mq ? 5 : 0);
-            if (!intra && (r.flags & H261B_MB_MC))
-                h += (c_vlc_mvd[dx < 0 ? -dx : dx] >> 8) + (c_vlc_mvd[dy < 0 ? -dy : dy] >> 8);
-            if (!intra && (r.flags & H261B_MB_COEFF))
-                h += c_vlc_cbp[r.cbp & 63] >> 8;
-            bad = mt < 0 || (!intra && (r.flags & H261B_MB_COEFF) && (r.cbp & 63) == 0);
-            bits = h + r.coef_bits;
-            sm.mb_plan[mi] = plan_pack(addr, mt < 0 ? 0 : mt, mq, dx, dy);
-        }
-        /* the 33rd macroblock, by every lane */
-        if (r32.flags != 0) {
-            const int addr = C ? 32 - (31 - __clz((int)C)) : 33;
-            const int qs = K ? qv32 : gq;
-            const bool intra = r32.type == H261B_MB_TYPE_INTRA;
-            const int mq = intra ? (r32.quant != qs) : (r32.quant != qs && (r32.flags & H261B_MB_COEFF));
-            const int mt = mtype_of(r32.type, r32.flags, mq);
-            const bool ok = (M >> 31) & 1u;
-            const int dx = wrap_mvd(r32.mvx - (ok ? mvx31 : 0)), dy = wrap_mvd(r32.mvy - (ok ? mvy31 : 0));
-            int h = (c_vlc_mba[addr] >> 8) + (mt >= 0 ? c_vlc_mtype_len[mt] : 0) + (mq ? 5 : 0);
-            if (!intra && (r32.flags & H261B_MB_MC))
-                h += (c_vlc_mvd[dx < 0 ? -dx : dx] >> 8) + (c_vlc_mvd[dy < 0 ? -dy : dy] >> 8);
-            if (!intra && (r32.flags & H261B_MB_COEFF))
-                h += c_vlc_cbp[r32.cbp & 63] >> 8;
-            bad |= mt < 0 || (!intra && (r32.flags & H261B_MB_COEFF) && (r32.cbp & 63) == 0);
-            bits32 = h + r32.coef_bits;
-            if (lane == 0)
-                sm.mb_plan[m32] = plan_pack(addr, mt < 0 ? 0 : mt, mq, dx, dy);
-        }
-        /* offsets within the GOB, after its 26-bit header */
-        int incl = bits;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(FULL, incl, o);
-            if (lane >= o)
-                incl += t;
-        }
-        const int sum32 = __shfl_sync(FULL, incl, 31);
-        sm.mb_off[mi] = 26 + incl - bits;
-        sm.mb_len[mi] = bits;
-        if (lane == 0) {
-            sm.mb_off[m32] = 26 + sum32;
-            sm.mb_len[m32] = bits32;
-            sm.gob_bits[g] = 26 + sum32 + bits32;
-        }
-        /* a size beyond the syntax's maximum would overrun the staging
-         * buffer: only a wrong count can produce one */
-        bad |= bits < 0 || bits > MB_MAX_BITS || bits32 < 0 || bits32 > MB_MAX_BITS;
-        if (__any_sync(FULL, bad) && lane == 0)
-            atomicExch(&sm.status, H261B_BITS_BAD_RECORD);
-    }
-    __syncthreads();
-
-    /* ---- B: GOB offsets after the 32-bit picture header */
-    if (tid == 0) {
-        int o = 32;
-        for (int g = 0; g < ngob; g++) {
-            sm.gob_off[g] = o;
-            o += sm.gob_bits[g];
-        }
-        sm.total_bits = o;
-        if ((int64_t)((o + 127) / 128) * 16 > S.bits_cap)
-            sm.status = H261B_BITS_OVERFLOW;
-    }
-    __syncthreads();
-    const int total = sm.total_bits;
-    if (sm.status != 0) {
-        if (tid == 0)
-            *S.pic_out = h261b_pic_info_t{ 0, -1, sm.status, gq };
-        return;
-    }
-    const int words = ((total + 127) / 128) * 4;   /* whole 16-byte units */
-    for (int i = tid; i < words; i += BS_THREADS)
-        S.bits_out[i] = 0u;
-    __syncthreads();
-
-    /* ---- C: headers and macroblocks */
-    if (tid == 0) {
-        /* PSC, TR, PTYPE (split 0, document camera 0, freeze release 1,
-         * source format, HI_RES bit 1, spare 1), PEI 0 */
-        const uint32_t ptype = (1u << 3) | ((cif ? 1u : 0u) << 2) | (1u << 1) | 1u;
-        S.bits_out[0] = bswap((16u << 12) | ((uint32_t)(S.frame_num & 31) << 7) | (ptype << 1));
-    }
-    if (tid < ngob) {
-        const uint32_t number = cif ? (uint32_t)tid + 1u : 2u * (uint32_t)tid + 1u;
-        put_bits_global(S.bits_out, sm.gob_off[tid], (1u << 10) | (number << 6) | ((uint32_t)gq << 1), 26);
-    }
-
     uint32_t *stage = sm.stage[warp];
-    int oob = 0;
-    for (int mb = warp; mb < nmb; mb += BS_WARPS) {
-        const int len = sm.mb_len[mb];
-        if (len == 0)
+    for (int i = lane; i < MB_WORDS; i += 32)
+        stage[i] = 0u;
+    __syncthreads();
+
+    const int slot = lane >> 3, j = lane & 7;
+    int lo, hi;
+    warp_range(n_work, lo, hi);
+    for (int w = lo; w < hi; w++) {
+        const uint32_t item = work[w];
+        const h261b_session_dev_t &S = sessions[item >> 12];
+        if (!S.bits_out)
             continue;
-        const int mbx = mb % S.mbw, mby = mb / S.mbw;
-        const int g = cif ? (mby / 3) * 2 + mbx / 11 : mby / 3;
-        const int64_t pos = (int64_t)sm.gob_off[g] + sm.mb_off[mb];
-        const int base = (int)(pos & 31);
-        const int nw = (base + len + 31) >> 5;
-        for (int i = lane; i < nw; i += 32)
-            stage[i] = 0u;
-        const h261b_mb_info_t r = info[mb];
-        const bool intra = r.type == H261B_MB_TYPE_INTRA;
-        const int cbp = intra ? 63 : ((r.flags & H261B_MB_COEFF) ? (r.cbp & 63) : 0);
-        __syncwarp();
+        const int mb = (int)(item & 4095u);
+        h261b_mb_info_t &rec = S.info_out[mb];
+        const int cbp = coded_blocks(rec);
+        const bool intra = rec.type == H261B_MB_TYPE_INTRA;
+        /* block b is coded when bit b of `order` is set */
+        const uint32_t order = __brev((uint32_t)cbp) >> 26;
+        const int nb = __popc(order);
 
-        /* header, lane 0 */
-        const uint32_t plan = sm.mb_plan[mb];
-        const int addr = plan & 63, mt = (plan >> 6) & 15, mq = (plan >> 10) & 1;
-        const int dx = (int)((plan >> 11) & 31) - 16, dy = (int)((plan >> 16) & 31) - 16;
-        int hpos = base;
-        {
-            const uint16_t e = c_vlc_mba[addr];
-            hpos += e >> 8;
-            if (lane == 0)
-                put_bits(stage, hpos - (e >> 8), e & 0xFF, e >> 8, oob);
-            const int ml = c_vlc_mtype_len[mt];
-            if (lane == 0)
-                put_bits(stage, hpos, 1u, ml, oob);
-            hpos += ml;
-            if (mq) {
-                if (lane == 0)
-                    put_bits(stage, hpos, (uint32_t)r.quant, 5, oob);
-                hpos += 5;
-            }
-            if (!intra && (r.flags & H261B_MB_MC)) {
-                uint32_t cx, cy;
-                int lx, ly;
-                mvd_code(dx, cx, lx);
-                mvd_code(dy, cy, ly);
-                if (lane == 0) {
-                    put_bits(stage, hpos, cx, lx, oob);
-                    put_bits(stage, hpos + lx, cy, ly, oob);
-                }
-                hpos += lx + ly;
-            }
-            if (!intra && cbp) {
-                const uint16_t e2 = c_vlc_cbp[cbp];
-                if (lane == 0)
-                    put_bits(stage, hpos, e2 & 0xFF, e2 >> 8, oob);
-                hpos += e2 >> 8;
-            }
-        }
-
-        /* blocks: luma 0-3 in one round, chroma 4-5 in the next; eight
-         * lanes per block, lane j of a block holds positions 8j..8j+7 of
-         * the transmission order */
-        const int slot = lane >> 3, j = lane & 7;
+        int pos = 0, oob = 0;
         const int8_t *lv = S.level_out + (size_t)mb * 384;
-        for (int round = 0; round < 2; round++) {
-            const int b = round * 4 + slot;
-            const bool here = b < 6 && ((cbp >> (5 - b)) & 1);
-            if (b < 6)
+        for (int r0 = 0; r0 < nb; r0 += 4) {
+            const bool here = r0 + slot < nb;
+            const int b = here ? (int)__fns(order, 0, r0 + slot + 1) : 0;
+            if (here)
                 *reinterpret_cast<uint2 *>(&sm.blk[warp][slot][j * 8]) =
                     *reinterpret_cast<const uint2 *>(lv + b * 64 + j * 8);
             __syncwarp();
@@ -371,10 +253,10 @@ __global__ void __launch_bounds__(BS_THREADS) bitstream_kernel(const h261b_sessi
                     continue;
                 const int v = c[i];
                 if (k == 0 && intra) {
-                    code[i] = (uint32_t)v & 0xFFu;
+                    code[i] = (uint32_t)v & 0xFFu;       /* the DC level as it is */
                     clen[i] = 8;
                 } else if (k == 0 && (v == 1 || v == -1)) {
-                    code[i] = v < 0 ? 3u : 2u;
+                    code[i] = v < 0 ? 3u : 2u;            /* first inter coefficient +-1 */
                     clen[i] = 2;
                 } else {
                     const int run = k - prev - 1;
@@ -384,6 +266,7 @@ __global__ void __launch_bounds__(BS_THREADS) bitstream_kernel(const h261b_sessi
                         code[i] = ((uint32_t)(e & 0xFF) << 1) | (v < 0 ? 1u : 0u);
                         clen[i] = (e >> 8) + 1;
                     } else {
+                        /* escape 0000 01, 6-bit run, 8-bit level */
                         code[i] = (1u << 14) | ((uint32_t)run << 8) | ((uint32_t)v & 0xFFu);
                         clen[i] = 20;
                     }
@@ -391,7 +274,7 @@ __global__ void __launch_bounds__(BS_THREADS) bitstream_kernel(const h261b_sessi
                 prev = k;
                 mine += clen[i];
             }
-            /* offsets of this lane's codes within the block */
+            /* offsets of this lane's codes within its block */
             int incl = mine;
 #pragma unroll
             for (int o = 1; o < 8; o <<= 1) {
@@ -401,8 +284,7 @@ __global__ void __launch_bounds__(BS_THREADS) bitstream_kernel(const h261b_sessi
             }
             const int last = __shfl_sync(FULL, incl, (slot << 3) | 7);
             const int btotal = here ? last + 2 : 0;
-            /* start of each block of the round after the earlier ones */
-            int bstart = hpos, rtotal = 0;
+            int bstart = pos, rtotal = 0;
 #pragma unroll
             for (int s2 = 0; s2 < 4; s2++) {
                 const int t = __shfl_sync(FULL, btotal, s2 << 3);
@@ -414,61 +296,266 @@ __global__ void __launch_bounds__(BS_THREADS) bitstream_kernel(const h261b_sessi
                 int p = bstart + incl - mine;
 #pragma unroll
                 for (int i = 0; i < 8; i++) {
-                    put_bits(stage, p, code[i], clen[i], oob);
+                    put_bits(stage, MB_WORDS, p, code[i], clen[i], oob);
                     p += clen[i];
                 }
                 if (j == 7)
-                    put_bits(stage, bstart + btotal - 2, 2u, 2, oob);   /* EOB */
+                    put_bits(stage, MB_WORDS, bstart + btotal - 2, 2u, 2, oob);   /* EOB */
             }
-            hpos += rtotal;
+            pos += rtotal;
             __syncwarp();
         }
-        const bool wrong = __any_sync(FULL, oob) || hpos - base != len || (pos >> 5) + nw > words;
-        if (wrong) {
-            if (lane == 0)
-                atomicExch(&sm.status, H261B_BITS_MISMATCH);
-            __syncwarp();
-            continue;
-        }
-
-        /* store; the first and the last word may be shared with the
-         * neighbouring macroblocks */
-        uint32_t *dst = S.bits_out + (pos >> 5);
+        oob = __any_sync(FULL, oob);
+        /* store the string and leave the staging words clear for the next */
+        uint32_t *dst = S.vlc_scratch + (size_t)mb * MB_WORDS;
+        const int nw = min((pos + 31) >> 5, MB_WORDS);
         for (int i = lane; i < nw; i += 32) {
-            const uint32_t x = bswap(stage[i]);
-            if (i == 0 || i == nw - 1)
-                atomicOr(&dst[i], x);
-            else
-                dst[i] = x;
+            dst[i] = stage[i];
+            stage[i] = 0u;
         }
+        if (lane == 0)
+            rec.coef_bits = oob ? -1 : pos;   /* -1 makes the layout refuse the picture */
         __syncwarp();
     }
+}
+
+/* ---- layout: one CTA per picture, a warp per GOB */
+__global__ void __launch_bounds__(VLC_THREADS) layout_kernel(const h261b_session_dev_t *sessions)
+{
+    const h261b_session_dev_t &S = sessions[blockIdx.x];
+    if (!S.bits_out)
+        return;
+    __shared__ int32_t rel[396];       /* MB position within its GOB */
+    __shared__ int32_t gob_bits[12];
+    __shared__ int64_t gob_start[13];
+    __shared__ int bad;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const bool cif = S.mbw == 22;
+    const int ngob = cif ? 12 : 3, nmb = S.mbw * S.mbh;
+    const int gq = S.quant;
+    const h261b_mb_info_t *info = S.info_out;
+    if (tid == 0)
+        bad = 0;
     __syncthreads();
 
-    /* ---- D: to the host arena */
-    const int bytes = (total + 7) >> 3;
-    const int padded = (bytes + 15) & ~15;
-    if (tid == 0) {
-        int off = -1;
-        if (sm.status != 0) {
-            *S.pic_out = h261b_pic_info_t{ 0, -1, sm.status, gq };
-            sm.host_off = -1;
-        } else {
-        if (host_arena) {
-            const uint32_t o = atomicAdd(&step->host_used, (uint32_t)padded);
-            if ((int64_t)o + padded <= host_cap)
-                off = (int)o;
+    for (int g = warp; g < ngob; g += VLC_WARPS) {
+        const int x0 = cif ? (g & 1) * 11 : 0, y0 = (cif ? g >> 1 : g) * 3;
+        const int mi = (y0 + lane / 11) * S.mbw + x0 + lane % 11;
+        const int m32 = (y0 + 2) * S.mbw + x0 + 10;
+        const h261b_mb_info_t r = info[mi];
+        const h261b_mb_info_t r32 = info[m32];
+        const uint32_t C = __ballot_sync(FULL, r.flags != 0);
+        const uint32_t K = __ballot_sync(FULL, (r.flags & H261B_MB_COEFF) != 0);
+        const uint32_t M = __ballot_sync(FULL, (r.flags & H261B_MB_MC) != 0);
+        const int pmx = __shfl_up_sync(FULL, (int)r.mvx, 1), pmy = __shfl_up_sync(FULL, (int)r.mvy, 1);
+        const uint32_t below = (1u << lane) - 1u, kb = K & below, cb = C & below;
+        /* quantiser in force: the last COEFF macroblock before, else GQUANT */
+        const int qv = __shfl_sync(FULL, (int)r.quant, kb ? 31 - __clz((int)kb) : lane);
+        const int qv32 = __shfl_sync(FULL, (int)r.quant, K ? 31 - __clz((int)K) : 0);
+        const int mvx31 = __shfl_sync(FULL, (int)r.mvx, 31), mvy31 = __shfl_sync(FULL, (int)r.mvy, 31);
+
+        int bits = 0, bits32 = 0, b = 0;
+        if (r.flags != 0) {
+            const int addr = cb ? lane - (31 - __clz((int)cb)) : lane + 1;
+            /* the predictor: the previous MB of the same MB row, coded with MC */
+            const bool ok = lane > 0 && lane % 11 != 0 && ((M >> (lane - 1)) & 1u);
+            const MbHeader hd = mb_header(r, addr, kb ? qv : gq, ok, pmx, pmy);
+            b |= hd.bad || r.coef_bits < 0 || r.coef_bits > MB_WORDS * 32;
+            bits = hd.bits + r.coef_bits;
+            S.vlc_plan[mi] = hd.plan;
         }
-        sm.host_off = off;
-        *S.pic_out = h261b_pic_info_t{ bytes, off, 0, gq };
+        if (r32.flags != 0) {
+            /* the 33rd macroblock, by every lane */
+            const int addr = C ? 32 - (31 - __clz((int)C)) : 33;
+            const MbHeader hd = mb_header(r32, addr, K ? qv32 : gq, (M >> 31) & 1u, mvx31, mvy31);
+            b |= hd.bad || r32.coef_bits < 0 || r32.coef_bits > MB_WORDS * 32;
+            bits32 = hd.bits + r32.coef_bits;
+            if (lane == 0)
+                S.vlc_plan[m32] = hd.plan;
         }
+        int incl = bits;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o)
+                incl += t;
+        }
+        const int sum32 = __shfl_sync(FULL, incl, 31);
+        rel[mi] = 26 + incl - bits;
+        if (lane == 0) {
+            rel[m32] = 26 + sum32;
+            gob_bits[g] = 26 + sum32 + bits32;
+        }
+        if (__any_sync(FULL, b) && lane == 0)
+            bad = 1;
     }
     __syncthreads();
-    if (sm.host_off >= 0) {
-        const uint4 *src = reinterpret_cast<const uint4 *>(S.bits_out);
-        uint4 *dst = reinterpret_cast<uint4 *>(host_arena + sm.host_off);
-        for (int i = tid; i < padded / 16; i += BS_THREADS)
-            dst[i] = src[i];
+    if (tid == 0) {
+        int64_t at = 32;                    /* after PSC, TR, PTYPE, PEI */
+        for (int g = 0; g < ngob; g++) {
+            gob_start[g] = at;
+            at += gob_bits[g];
+        }
+        gob_start[ngob] = at;
+    }
+    __syncthreads();
+    const int64_t total = gob_start[ngob];
+    const int64_t words = ((total + 127) / 128) * 4;   /* whole 16-byte units */
+    const int status = bad ? H261B_BITS_BAD_RECORD : (words * 4 > S.bits_cap ? H261B_BITS_OVERFLOW : 0);
+    if (status == 0) {
+        for (int i = tid; i < nmb; i += VLC_THREADS) {
+            const int mbx = i % S.mbw, mby = i / S.mbw;
+            const int g = cif ? (mby / 3) * 2 + mbx / 11 : mby / 3;
+            S.vlc_pos[i] = (int32_t)(gob_start[g] + rel[i]);
+        }
+        for (int64_t i = tid; i < words; i += VLC_THREADS)
+            S.bits_out[i] = 0u;
+    }
+    __syncthreads();
+    int oob = 0;
+    if (status == 0) {
+        if (tid == 0) {
+            /* PSC, TR, PTYPE (split 0, document camera 0, freeze release 1,
+             * source format, HI_RES bit 1, spare 1), PEI 0 */
+            const uint32_t ptype = (1u << 3) | ((cif ? 1u : 0u) << 2) | (1u << 1) | 1u;
+            S.bits_out[0] = bswap((16u << 12) | ((uint32_t)(S.frame_num & 31) << 7) | (ptype << 1));
+        }
+        if (tid < ngob) {
+            /* GOB header: GBSC, GN, GQUANT, GEI */
+            const uint32_t number = cif ? (uint32_t)tid + 1u : 2u * (uint32_t)tid + 1u;
+            put_bits_pic(S.bits_out, words, gob_start[tid], (1u << 10) | (number << 6) | ((uint32_t)gq << 1), 26,
+                         oob);
+        }
+    }
+    const int any_oob = __syncthreads_or(oob);
+    if (tid == 0) {
+        S.vlc_total[0] = (int32_t)total;
+        S.vlc_total[1] = status != 0 ? status : (any_oob ? H261B_BITS_MISMATCH : 0);
+    }
+}
+
+/* ---- pack: headers and coefficient strings into the picture */
+__global__ void __launch_bounds__(VLC_THREADS) pack_kernel(const h261b_session_dev_t *sessions,
+                                                           const uint32_t *work, int32_t n_work)
+{
+    const int lane = threadIdx.x & 31;
+    int lo, hi;
+    warp_range(n_work, lo, hi);
+    for (int w = lo; w < hi; w++) {
+        const uint32_t item = work[w];
+        const h261b_session_dev_t &S = sessions[item >> 12];
+        if (!S.bits_out)
+            continue;
+        const int mb = (int)(item & 4095u);
+        const h261b_mb_info_t r = S.info_out[mb];
+        if (r.flags == 0)
+            continue;
+        const int total = S.vlc_total[0];
+        const int64_t words = ((int64_t)(total + 127) / 128) * 4;
+        /* a layout that does not fit the slot is refused, whatever wrote it */
+        if (S.vlc_total[1] != 0 || total < 0 || words * 4 > S.bits_cap)
+            continue;
+        int oob = 0;
+        const int64_t pos = S.vlc_pos[mb];
+        const uint32_t plan = S.vlc_plan[mb];
+        const int addr = plan & 63, mt = (plan >> 6) & 15, mq = (plan >> 10) & 1;
+        const int dx = (int)((plan >> 11) & 31) - 16, dy = (int)((plan >> 16) & 31) - 16;
+        const bool intra = r.type == H261B_MB_TYPE_INTRA;
+        const int cbp = coded_blocks(r);
+        /* the header as one MSB-first value of at most 57 bits */
+        uint64_t hv;
+        int hl;
+        {
+            const uint16_t e = c_vlc_mba[addr];
+            hv = e & 0xFF;
+            hl = e >> 8;
+            const int ml = c_vlc_mtype_len[mt];
+            hv = (hv << ml) | 1u;
+            hl += ml;
+            if (mq) {
+                hv = (hv << 5) | (uint32_t)r.quant;
+                hl += 5;
+            }
+            if (!intra && (r.flags & H261B_MB_MC)) {
+                uint32_t cx, cy;
+                int lx, ly;
+                mvd_code(dx, cx, lx);
+                mvd_code(dy, cy, ly);
+                hv = (((hv << lx) | cx) << ly) | cy;
+                hl += lx + ly;
+            }
+            if (!intra && cbp) {
+                const uint16_t e2 = c_vlc_cbp[cbp];
+                hv = (hv << (e2 >> 8)) | (e2 & 0xFF);
+                hl += e2 >> 8;
+            }
+        }
+        if (lane == 0) {
+            if (hl > 32) {
+                put_bits_pic(S.bits_out, words, pos, (uint32_t)(hv >> 32), hl - 32, oob);
+                put_bits_pic(S.bits_out, words, pos + (hl - 32), (uint32_t)hv, 32, oob);
+            } else {
+                put_bits_pic(S.bits_out, words, pos, (uint32_t)hv, hl, oob);
+            }
+        }
+        /* the coefficient bits, shifted into place */
+        const int nbits = r.coef_bits;
+        if (nbits > 0) {
+            const int64_t q = pos + hl;
+            const int sh = (int)(q & 31);
+            const int64_t w0 = q >> 5;
+            const int nout = (sh + nbits + 31) >> 5, nin = (nbits + 31) >> 5;
+            const uint32_t *src = S.vlc_scratch + (size_t)mb * MB_WORDS;
+            if (w0 < 0 || w0 + nout > words || nin > MB_WORDS) {
+                oob = 1;
+            } else {
+                for (int i = lane; i < nout; i += 32) {
+                    const uint32_t hi = i < nin ? src[i] : 0u;
+                    const uint32_t lo = i > 0 ? src[i - 1] : 0u;
+                    const uint32_t x = sh ? ((hi >> sh) | (lo << (32 - sh))) : hi;
+                    uint32_t *d = S.bits_out + w0 + i;
+                    if (i == 0 || i == nout - 1)
+                        atomicOr(d, bswap(x));
+                    else
+                        *d = bswap(x);
+                }
+            }
+        }
+        if (__any_sync(FULL, oob) && lane == 0)
+            atomicExch(&S.vlc_total[1], H261B_BITS_MISMATCH);
+    }
+}
+
+/* ---- copy: each picture into the host arena */
+__global__ void __launch_bounds__(VLC_THREADS) copy_kernel(const h261b_session_dev_t *sessions,
+                                                           h261b_step_dev_t *step, uint8_t *host_arena,
+                                                           int64_t host_cap)
+{
+    const h261b_session_dev_t &S = sessions[blockIdx.x];
+    if (!S.bits_out)
+        return;
+    __shared__ int off;
+    const int total = S.vlc_total[0];
+    const int64_t words = ((int64_t)(total + 127) / 128) * 4;
+    const int st = (total < 0 || words * 4 > S.bits_cap) ? H261B_BITS_OVERFLOW : S.vlc_total[1];
+    const int bytes = (total + 7) >> 3;
+    const int padded = (bytes + 15) & ~15;
+    if (threadIdx.x == 0) {
+        int o = -1;
+        if (st == 0 && host_arena) {
+            const uint32_t a = atomicAdd(&step->host_used, (uint32_t)padded);
+            if ((int64_t)a + padded <= host_cap)
+                o = (int)a;
+        }
+        off = o;
+        *S.pic_out = h261b_pic_info_t{ st == 0 ? bytes : 0, o, st, S.quant };
+    }
+    __syncthreads();
+    if (off >= 0) {
+        const uint4 *s4 = reinterpret_cast<const uint4 *>(S.bits_out);
+        uint4 *d4 = reinterpret_cast<uint4 *>(host_arena + off);
+        for (int i = threadIdx.x; i < padded / 16; i += VLC_THREADS)
+            d4[i] = s4[i];
     }
 }
 
@@ -477,23 +564,37 @@ __global__ void __launch_bounds__(BS_THREADS) bitstream_kernel(const h261b_sessi
 
 using namespace h261b;
 
-extern "C" int64_t h261b_bits_slot_bytes(int32_t w, int32_t h)
+extern "C" h261b_bits_layout_t h261b_bits_layout(int32_t w, int32_t h)
 {
+    h261b_bits_layout_t l = { 0, 0, 0, 0, 0, 0 };
     const bool cif = w == 352 && h == 288, qcif = w == 176 && h == 144;
     if (!cif && !qcif)
-        return 0;
-    const int64_t nmb = (w / 16) * (h / 16), ngob = cif ? 12 : 3;
-    const int64_t bits = 32 + 26 * ngob + nmb * MB_MAX_BITS;
-    return ((bits + 127) / 128) * 16;
+        return l;
+    const int64_t nmb = (int64_t)(w / 16) * (h / 16), ngob = cif ? 12 : 3;
+    const int64_t pic_bits = 32 + 26 * ngob + nmb * (MB_HDR_MAX + MB_WORDS * 32);
+    auto al = [](int64_t x) { return (x + 255) / 256 * 256; };
+    l.picture = 0;
+    l.scratch = al(((pic_bits + 127) / 128) * 16);
+    l.pos = l.scratch + al(nmb * MB_WORDS * 4);
+    l.plan = l.pos + al(nmb * 4);
+    l.total = l.plan + al(nmb * 4);
+    l.bytes = l.total + 256;
+    return l;
 }
 
-extern "C" int h261b_launch_bitstream(const h261b_session_dev_t *sessions_dev, int32_t n_sessions,
-                                      h261b_step_dev_t *step, uint8_t *host_arena_dev, int64_t host_cap,
-                                      void *stream)
+extern "C" int64_t h261b_bits_slot_bytes(int32_t w, int32_t h) { return h261b_bits_layout(w, h).bytes; }
+
+extern "C" int h261b_launch_bitstream(h261b_session_dev_t *sessions_dev, int32_t n_sessions, const uint32_t *work_dev,
+                                      int32_t n_work, h261b_step_dev_t *step, uint8_t *host_arena_dev,
+                                      int64_t host_cap, int32_t sm_count, void *stream)
 {
-    if (n_sessions <= 0)
+    if (n_work <= 0 || n_sessions <= 0)
         return 0;
-    bitstream_kernel<<<n_sessions, BS_THREADS, 0, (cudaStream_t)stream>>>(sessions_dev, step, host_arena_dev,
-                                                                          host_cap);
+    const int ctas = (int)std::min<int64_t>((n_work + 4 * VLC_WARPS - 1) / (4 * VLC_WARPS), (int64_t)sm_count * 4);
+    cudaStream_t st = (cudaStream_t)stream;
+    codes_kernel<<<ctas, VLC_THREADS, 0, st>>>(sessions_dev, work_dev, n_work);
+    layout_kernel<<<n_sessions, VLC_THREADS, 0, st>>>(sessions_dev);
+    pack_kernel<<<ctas, VLC_THREADS, 0, st>>>(sessions_dev, work_dev, n_work);
+    copy_kernel<<<n_sessions, VLC_THREADS, 0, st>>>(sessions_dev, step, host_arena_dev, host_cap);
     return (int)cudaGetLastError();
 }

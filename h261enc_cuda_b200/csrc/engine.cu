@@ -183,10 +183,11 @@ struct Session {
     int rec_cur = 0;               /* holds the latest reconstruction     */
     h261b_denoise_dev_t *dn = nullptr;
     size_t slot_bytes = 0;
-    /* bitstream: one device slot per step parity */
+    /* bitstream: one device block per step parity (picture, MB scratch,
+     * positions, header plans, picture size) */
     bool bitstream = false;
-    uint32_t *bits_slot[2] = { nullptr, nullptr };
-    size_t bits_slot_bytes = 0;
+    uint8_t *bits_base[2] = { nullptr, nullptr };
+    h261b_bits_layout_t bits_lay = {};
     std::vector<uint8_t> bits_spill;   /* a picture the host arena missed */
     /* queued picture: in the upload arena, or already in device memory */
     bool queued = false;
@@ -220,6 +221,8 @@ struct h261b_engine_s {
     cudaEvent_t kernel_done[2] = { nullptr, nullptr };
     cudaEvent_t step_done[2] = { nullptr, nullptr };
     cudaEvent_t k_start[2] = { nullptr, nullptr }, k_end[2] = { nullptr, nullptr };
+    cudaEvent_t b_end[2] = { nullptr, nullptr };   /* after the bitstream kernel */
+    bool step_bits_ran[2] = { false, false };
     bool in_flight[2] = { false, false };
     int64_t step_mbs[2] = { 0, 0 };   /* MB records of the step in each arena */
     int64_t last_h2d = 0, last_d2h = 0;  /* bytes copied by the last step */
@@ -329,7 +332,8 @@ extern "C" int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engin
              cudaEventCreateWithFlags(&e->h2d_done[p], cudaEventDisableTiming) == cudaSuccess &&
              cudaEventCreateWithFlags(&e->kernel_done[p], cudaEventDisableTiming) == cudaSuccess &&
              cudaEventCreateWithFlags(&e->step_done[p], cudaEventDisableTiming) == cudaSuccess &&
-             cudaEventCreate(&e->k_start[p]) == cudaSuccess && cudaEventCreate(&e->k_end[p]) == cudaSuccess;
+             cudaEventCreate(&e->k_start[p]) == cudaSuccess && cudaEventCreate(&e->k_end[p]) == cudaSuccess &&
+             cudaEventCreate(&e->b_end[p]) == cudaSuccess;
     }
     if (!ok) {
         set_error("h261b_engine_create: device setup failed: %s", cudaGetErrorString(cudaGetLastError()));
@@ -370,6 +374,7 @@ extern "C" int h261b_engine_destroy(h261b_engine_t *e)
         cudaEventDestroy(e->step_done[p]);
         cudaEventDestroy(e->k_start[p]);
         cudaEventDestroy(e->k_end[p]);
+        cudaEventDestroy(e->b_end[p]);
         if (e->stream[p])
             cudaStreamDestroy(e->stream[p]);
     }
@@ -441,9 +446,9 @@ extern "C" int h261b_session_open(h261b_engine_t *e, const h261b_session_config_
         const size_t sb = align_up((size_t)h261b_bits_slot_bytes(c->width, c->height), 256);
         uint8_t *b0 = base + h261b_session_bytes(c->width, c->height);
         s.bitstream = true;
-        s.bits_slot_bytes = sb;
-        s.bits_slot[0] = (uint32_t *)b0;
-        s.bits_slot[1] = (uint32_t *)(b0 + sb);
+        s.bits_lay = h261b_bits_layout(c->width, c->height);
+        s.bits_base[0] = b0;
+        s.bits_base[1] = b0 + sb;
     }
     /* the first reference is black like the reference's zeroed frame
      * (h261_main.c:155-157); denoise state starts at zero
@@ -458,6 +463,8 @@ extern "C" int h261b_session_open(h261b_engine_t *e, const h261b_session_config_
     dn0.denoise = c->denoise;
     cudaStream_t st = e->stream[e->next_step & 1];
     H261B_CUDA_TRY(cudaMemsetAsync(base, 0, 2 * s.lay.bytes, st));
+    for (int q = 0; q < 2 && s.bitstream; q++)
+        H261B_CUDA_TRY(cudaMemsetAsync(s.bits_base[q] + s.bits_lay.total, 0, 256, st));
     H261B_CUDA_TRY(cudaMemcpyAsync(s.dn, &dn0, sizeof(dn0), cudaMemcpyHostToDevice, st));
     s.open = true;
     e->open_count++;
@@ -800,10 +807,16 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
         r.has_bits = s.bitstream;
         r.pic_off = pic_base + k * sizeof(h261b_pic_info_t);
         if (s.bitstream) {
-            d.bits_out = s.bits_slot[p];
-            d.bits_cap = (int32_t)s.bits_slot_bytes;
+            uint8_t *bb = s.bits_base[p];
+            const h261b_bits_layout_t &L = s.bits_lay;
+            d.bits_out = (uint32_t *)(bb + L.picture);
+            d.bits_cap = (int32_t)(L.scratch - L.picture);
             d.frame_num = s.frame_index;
             d.pic_out = (h261b_pic_info_t *)(rm.dev + r.pic_off);
+            d.vlc_scratch = (uint32_t *)(bb + L.scratch);
+            d.vlc_pos = (int32_t *)(bb + L.pos);
+            d.vlc_plan = (uint32_t *)(bb + L.plan);
+            d.vlc_total = (int32_t *)(bb + L.total);
             n_bits++;
         }
         for (int32_t m = 0; m < s.nmb; m++)
@@ -835,13 +848,16 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
     if (n_bits) {
         if ((rc = e->bits[p].reserve(e->bits_want)))
             return rc;
-        lr = h261b_launch_bitstream(desc_dev, (int32_t)n, (h261b_step_dev_t *)dm.dev, e->bits[p].dev,
-                                    (int64_t)e->bits[p].cap, st);
+        lr = h261b_launch_bitstream((h261b_session_dev_t *)(dm.dev + desc_off), (int32_t)n,
+                                    (const uint32_t *)(dm.dev + work_off), n_work, (h261b_step_dev_t *)dm.dev,
+                                    e->bits[p].dev, (int64_t)e->bits[p].cap, e->sm_count, st);
         if (lr != 0) {
             set_error("bitstream launch failed: %s", cudaGetErrorString((cudaError_t)lr));
             return H261B_ERR_CUDA;
         }
+        H261B_CUDA_TRY(cudaEventRecord(e->b_end[p], st));
     }
+    e->step_bits_ran[p] = n_bits > 0;
     /* records and picture records always, levels when asked for */
     const size_t d2h = e->cfg.levels_to_host ? res_off : levels_base;
     H261B_CUDA_TRY(cudaMemcpyAsync(rm.host, rm.dev, d2h, cudaMemcpyDeviceToHost, st));
@@ -947,7 +963,7 @@ extern "C" int h261b_session_result(h261b_engine_t *e, int32_t id, h261b_frame_r
              * next); later steps get a larger arena */
             s->bits_spill.resize((size_t)pi.bytes);
             cudaSetDevice(e->cfg.device);
-            H261B_CUDA_TRY(cudaMemcpy(s->bits_spill.data(), s->bits_slot[p], (size_t)pi.bytes,
+            H261B_CUDA_TRY(cudaMemcpy(s->bits_spill.data(), s->bits_base[p] + s->bits_lay.picture, (size_t)pi.bytes,
                                       cudaMemcpyDeviceToHost));
             out->bits = s->bits_spill.data();
             out->bits_bytes = pi.bytes;
@@ -1047,6 +1063,62 @@ extern "C" int h261b_engine_last_copy_bytes(h261b_engine_t *e, int64_t *h2d, int
         return H261B_ERR_ARG;
     *h2d = e->last_h2d;
     *d2h = e->last_d2h;
+    return H261B_OK;
+}
+
+extern "C" int h261b_engine_last_bits_ms(h261b_engine_t *e, float *ms)
+{
+    if (!e || !ms || e->next_step == 0)
+        return H261B_ERR_ARG;
+    const int p = (int)((e->next_step - 1) & 1);
+    *ms = 0.f;
+    if (!e->step_bits_ran[p])
+        return H261B_OK;
+    H261B_CUDA_TRY(cudaEventSynchronize(e->b_end[p]));
+    H261B_CUDA_TRY(cudaEventElapsedTime(ms, e->k_end[p], e->b_end[p]));
+    return H261B_OK;
+}
+
+extern "C" int h261b_engine_step_pictures(h261b_engine_t *e, int32_t cap, h261b_picture_t *out, int32_t *count,
+                                          const uint8_t **arena, int64_t *arena_bytes)
+{
+    clear_error();
+    if (!e || !count || (cap > 0 && !out) || cap < 0)
+        return H261B_ERR_ARG;
+    *count = 0;
+    if (arena)
+        *arena = nullptr;
+    if (arena_bytes)
+        *arena_bytes = 0;
+    if (e->done_step < 0)
+        return H261B_OK;
+    const int p = (int)(e->done_step & 1);
+    const Mirror &rm = e->results[p];
+    int64_t span = 0;
+    int32_t n = 0;
+    for (size_t i = 0; i < e->sessions.size(); i++) {
+        const Session &s = e->sessions[i];
+        const Result &r = s.res[p];
+        if (!s.open || !r.has_bits || r.step != e->done_step)
+            continue;
+        const h261b_pic_info_t &pi = *(const h261b_pic_info_t *)(rm.host + r.pic_off);
+        if (pi.status == 0 && pi.host_off >= 0)
+            span = std::max<int64_t>(span, (int64_t)pi.host_off + ((pi.bytes + 15) & ~15));
+        if (n < cap) {
+            h261b_picture_t &o = out[n];
+            o.session_id = (int32_t)i;
+            o.frame_index = r.frame;
+            o.bytes = pi.status == 0 ? pi.bytes : 0;
+            o.status = pi.status == 0 ? (pi.host_off >= 0 ? 0 : 1) : H261B_ERR_STATE;
+            o.bits = (pi.status == 0 && pi.host_off >= 0) ? e->bits[p].host + pi.host_off : nullptr;
+        }
+        n++;
+    }
+    *count = n;
+    if (arena)
+        *arena = e->bits[p].host;
+    if (arena_bytes)
+        *arena_bytes = span;
     return H261B_OK;
 }
 

@@ -91,11 +91,21 @@ typedef struct {
     int8_t *level_out;            /* [nmb][6][64], per block column-major
                                      ([u][v]); an intra DC stored as uint8   */
     /* bitstream of the picture (QCIF / CIF sessions that write one) */
-    uint32_t *bits_out;           /* device slot, 16-byte aligned, NULL = none */
+    uint32_t *bits_out;           /* picture bytes, 16-byte aligned; NULL = no
+                                     bitstream                               */
     int32_t bits_cap;             /* bytes in bits_out                       */
     int32_t frame_num;            /* temporal reference = frame_num & 31     */
     h261b_pic_info_t *pic_out;
+    uint32_t *vlc_scratch;        /* per MB: its coefficient bits, MSB first,
+                                     H261B_VLC_MB_WORDS words apart          */
+    int32_t *vlc_pos;             /* per MB: bit position in the picture     */
+    uint32_t *vlc_plan;           /* per MB: header fields                   */
+    int32_t *vlc_total;           /* [0] picture bits, [1] status            */
 } h261b_session_dev_t;
+
+/* coefficient bits of one MB at most: six blocks of an 8-bit DC or a first
+ * code, 63 escapes of 20 bits and an EOB */
+#define H261B_VLC_MB_WORDS 240
 
 /* phases a launch runs for each MB */
 #define H261B_PHASE_ME      1     /* search + cost evaluation               */
@@ -110,14 +120,22 @@ int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const uint32_t *w
                       int32_t n_work, int32_t phases, int32_t warps_per_cta, int32_t max_ctas,
                       void *stream);
 int h261b_set_quant_table(void);
-/* one CTA per session of the descriptor array that has bits_out: writes the
- * picture into bits_out, then into the host arena (device-mapped pinned
+/* the bitstream of every work item's session that has bits_out: four
+ * launches (coefficient codes and packing over the step's work list,
+ * layout and the host copy per session);
+ * the picture ends in bits_out and in the host arena (device-mapped pinned
  * memory, host_cap bytes) at an offset drawn from step->host_used */
-int h261b_launch_bitstream(const h261b_session_dev_t *sessions_dev, int32_t n_sessions, h261b_step_dev_t *step,
-                           uint8_t *host_arena_dev, int64_t host_cap, void *stream);
-/* device slot bytes a w x h picture's bitstream may need (0: no bitstream
- * for this size) */
+int h261b_launch_bitstream(h261b_session_dev_t *sessions_dev, int32_t n_sessions, const uint32_t *work_dev,
+                           int32_t n_work, h261b_step_dev_t *step, uint8_t *host_arena_dev, int64_t host_cap,
+                           int32_t sm_count, void *stream);
+/* device bytes per step parity a w x h session's bitstream needs: picture
+ * bytes, MB scratch and offsets (0: no bitstream for this size), and where
+ * each part starts in that block */
 int64_t h261b_bits_slot_bytes(int32_t w, int32_t h);
+typedef struct {
+    int64_t picture, scratch, pos, plan, total, bytes;
+} h261b_bits_layout_t;
+h261b_bits_layout_t h261b_bits_layout(int32_t w, int32_t h);
 #ifdef __cplusplus
 }
 #endif

@@ -43,7 +43,6 @@
 #include <mutex>
 
 #include "h261b_device.h"
-#include "vlc_tables.h"
 
 namespace {
 
@@ -488,7 +487,7 @@ __device__ __forceinline__ int hfilt(uint2 v, int c)
 template <int FMAD>
 __device__ __forceinline__ uint32_t encdec_pass(float (*tb)[72], const StageBuf &s, const h261b_session_dev_t &S,
                                                 int mb, int mbx, int mby, const MbDecision &m, int quant,
-                                                bool luma_pass, int lane, int32_t colsum[8], int32_t &vlc_bits)
+                                                bool luma_pass, int lane, int32_t colsum[8])
 {
     const bool active = luma_pass || lane < 16;
     const int slot = lane >> 3, r = lane & 7;
@@ -609,56 +608,6 @@ __device__ __forceinline__ uint32_t encdec_pass(float (*tb)[72], const StageBuf 
     acc += __shfl_xor_sync(FULL, acc, 4);
     const bool coded = active && acc > 2;
     const uint32_t cbp = __reduce_or_sync(FULL, coded ? (uint32_t)H261B_CBP_BIT(b) : 0u);
-
-    /* bits this pass's coded blocks take in the bitstream (TCOEFF codes,
-     * intra DC, EOB; src/h261_macroblock.c:5-92), for the bitstream
-     * writer's offsets: the block's nonzero levels as a 64-bit mask in
-     * transmission order give every level its run */
-    if (S.bits_out) {
-        uint32_t mlo = 0, mhi = 0;
-        int zz[8];
-#pragma unroll
-        for (int v = 0; v < 8; v++) {
-            zz[v] = h261b::zigzag_index(v, c);
-            if (active && lev[v] != 0) {
-                if (zz[v] < 32)
-                    mlo |= 1u << zz[v];
-                else
-                    mhi |= 1u << (zz[v] - 32);
-            }
-        }
-#pragma unroll
-        for (int o = 1; o < 8; o <<= 1) {
-            mlo |= __shfl_xor_sync(FULL, mlo, o);
-            mhi |= __shfl_xor_sync(FULL, mhi, o);
-        }
-        const uint64_t mask = ((uint64_t)mhi << 32) | mlo;
-        int bits = 0;
-        if (active) {
-#pragma unroll
-            for (int v = 0; v < 8; v++) {
-                if (lev[v] == 0)
-                    continue;
-                const int k = zz[v];
-                if (k == 0 && intra) {
-                    bits += 8;
-                } else if (k == 0 && (lev[v] == 1 || lev[v] == -1)) {
-                    bits += 2;
-                } else {
-                    const uint64_t below = mask & ((1ull << k) - 1ull);
-                    const int prev = below ? 63 - __clzll((long long)below) : -1;
-                    bits += h261b::tcoeff_bits(k - prev - 1, lev[v]);
-                }
-            }
-        }
-        bits += __shfl_xor_sync(FULL, bits, 1);
-        bits += __shfl_xor_sync(FULL, bits, 2);
-        bits += __shfl_xor_sync(FULL, bits, 4);
-        int blk = (active && (intra || coded)) ? bits + 2 : 0;
-        blk += __shfl_xor_sync(FULL, blk, 8);
-        blk += __shfl_xor_sync(FULL, blk, 16);
-        vlc_bits += blk;   /* one lane of each of the pass's blocks summed */
-    }
 
     /* denoise statistics: sum the same coefficient position over blocks */
 #pragma unroll
@@ -939,9 +888,8 @@ __global__ void __launch_bounds__(256) step_kernel(const h261b_session_dev_t *__
             if (S.md_in && !(phases & H261B_PHASE_MD))
                 quant += S.md_in[mb].i_quantiser_adjust;
             quant = min(31, max(1, quant)); /* gpu_device.cu:625-627 */
-            int32_t vlc_bits = 0;
-            uint32_t cbp = encdec_pass<FMAD>(sm.t, b, S, mb, mbx, mby, m, quant, true, lane, colsum, vlc_bits);
-            cbp |= encdec_pass<FMAD>(sm.t, b, S, mb, mbx, mby, m, quant, false, lane, colsum, vlc_bits);
+            uint32_t cbp = encdec_pass<FMAD>(sm.t, b, S, mb, mbx, mby, m, quant, true, lane, colsum);
+            cbp |= encdec_pass<FMAD>(sm.t, b, S, mb, mbx, mby, m, quant, false, lane, colsum);
             run_n++;
 
             const int flags = m.flags | (cbp ? H261B_MB_COEFF : 0);
@@ -967,7 +915,7 @@ __global__ void __launch_bounds__(256) step_kernel(const h261b_session_dev_t *__
                     inf.mvx = (int8_t)m.mvx;
                     inf.mvy = (int8_t)m.mvy;
                     inf.cost = m.cost;
-                    inf.coef_bits = vlc_bits;
+                    inf.coef_bits = 0;   /* the bitstream kernels fill it in */
                     S.info_out[mb] = inf;
                 }
             }

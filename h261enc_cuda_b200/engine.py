@@ -173,6 +173,24 @@ class Engine:
         bits = ctypes.string_at(r.bits, r.bits_bytes) if r.bits else None
         return FrameResult(r.frame_index, r.frame_type, r.quant, mbs, lv, bits, r.bits_status)
 
+    def last_bits_ms(self) -> float:
+        ms = ctypes.c_float()
+        check(_lib.core().h261b_engine_last_bits_ms(self._h, ctypes.byref(ms)), "h261b_engine_last_bits_ms")
+        return ms.value
+
+    def step_pictures(self, cap: int = 4096):
+        """(PICTURE_DTYPE array, host arena span as a uint8 view) of the
+        latest completed step's bitstream output."""
+        out = np.zeros(cap, _lib.PICTURE_DTYPE)
+        n = ctypes.c_int32()
+        base, used = ctypes.c_void_p(), ctypes.c_int64()
+        check(_lib.core().h261b_engine_step_pictures(self._h, cap, out.ctypes.data, ctypes.byref(n),
+                                                     ctypes.byref(base), ctypes.byref(used)),
+              "h261b_engine_step_pictures")
+        span = (np.ctypeslib.as_array((ctypes.c_uint8 * used.value).from_address(base.value))
+                if used.value else np.empty(0, np.uint8))
+        return out[:min(n.value, cap)], span
+
     def step_bits(self):
         """(bytes, pictures) of bitstream the latest completed step wrote."""
         b, n = ctypes.c_int64(), ctypes.c_int32()

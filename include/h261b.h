@@ -185,6 +185,25 @@ int h261b_engine_step_records(h261b_engine_t *e, const h261b_mb_result_t **recor
  * open sessions that write one. */
 int h261b_engine_step_bits(h261b_engine_t *e, int64_t *bytes, int32_t *pictures);
 
+/* one picture of a step's bitstream output */
+typedef struct {
+    int32_t session_id;
+    int32_t frame_index;
+    int32_t bytes;
+    int32_t status;           /* 0: bits points into the host arena; 1: the
+                                 arena was full, h261b_session_result() reads
+                                 it from the device; < 0: no bitstream        */
+    const uint8_t *bits;
+} h261b_picture_t;
+
+/* Every picture the latest completed step wrote as a bitstream, in
+ * ascending session id: up to cap entries into out, *count = all of them.
+ * *arena / *arena_bytes: the host arena holding them (each picture on a
+ * 16-byte boundary) and the bytes of it in use, for callers that move a
+ * step's output in one copy.  Valid until the step after next is issued. */
+int h261b_engine_step_pictures(h261b_engine_t *e, int32_t cap, h261b_picture_t *out, int32_t *count,
+                               const uint8_t **arena, int64_t *arena_bytes);
+
 /* Copy the session's latest reconstruction (packed planes) to the host. */
 int h261b_session_recon(h261b_engine_t *e, int32_t session_id, uint8_t *y, uint8_t *cb, uint8_t *cr);
 
@@ -192,8 +211,10 @@ int h261b_session_recon(h261b_engine_t *e, int32_t session_id, uint8_t *y, uint8
  * reference's GOB / macroblock writers read); mbs[] gets num_mb entries. */
 int h261b_result_to_abi(const h261b_frame_result_t *r, int32_t width, h261_macroblock_t *mbs);
 
-/* Device time of the last step's kernel in milliseconds (CUDA events). */
+/* Device time of the last step's encode kernel, and of its bitstream
+ * kernel (0 without bitstream sessions), in milliseconds (CUDA events). */
 int h261b_engine_last_kernel_ms(h261b_engine_t *e, float *ms);
+int h261b_engine_last_bits_ms(h261b_engine_t *e, float *ms);
 /* Bytes the last step copied host->device (descriptors, work list,
  * pictures) and device->host (records, picture records, levels when copied;
  * the bitstream bytes, which the device writes into mapped host memory,
