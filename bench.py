@@ -246,16 +246,17 @@ def device_clips(streams, clip_len, device):
 
 class Runner:
     """Keeps the workload's slots full: a stream that reaches its length is
-    replaced by a new session (same geometry and QUANT) and closed once its
-    last picture has been read (``retire``).  The engine returns a closed
-    session's device slot to its pool when the steps in flight that use it
-    have completed, so nothing drains here."""
+    replaced by a new session (same geometry and QUANT) and closed once the
+    step with its last picture has been read (``retire``).  The engine
+    returns a closed session's device slot to its pool when the steps in
+    flight that use it have completed, so nothing drains here."""
 
     def __init__(self, engine, streams, pools):
         self.e, self.streams, self.pools = engine, streams, pools
         self.sids = [engine.open(s.width, s.height, s.quant, bitstream=1) for s in streams]
         self.pos = [0] * len(streams)
-        self.ending = []
+        self.queued = 0            # steps queued so far
+        self.ending = []           # (session, step holding its last picture)
         # host pictures: one contiguous (clip, W*H*3/2) array per stream
         self.base = np.array([p[1].ctypes.data for p in pools], np.uint64)
         self.fbytes = np.array([p[1].shape[1] for p in pools], np.uint64)
@@ -266,29 +267,35 @@ class Runner:
         idx = np.empty(len(self.streams), np.uint64)
         for k, s in enumerate(self.streams):
             if self.pos[k] >= s.length:
-                self.ending.append(self.sids[k])
+                self.ending.append((self.sids[k], self.queued - 1))
                 self.sids[k] = self.e.open(s.width, s.height, s.quant, bitstream=1)
                 self.pos[k] = 0
             idx[k] = workloads.clip_index(self.pos[k], CLIP_LEN)
             self.pos[k] += 1
+        self.queued += 1
         return idx
 
-    def retire(self):
-        """Close the streams whose last picture was in the step just read."""
-        for sid in self.ending:
-            self.e.close(sid)
-        self.ending = []
+    def retire(self, read_step):
+        """Close the streams whose last picture was in a step already read."""
+        keep = []
+        for sid, last in self.ending:
+            if last <= read_step:
+                self.e.close(sid)
+            else:
+                keep.append((sid, last))
+        self.ending = keep
 
     def queue_device(self):
         idx = self._advance()
         for k, sid in enumerate(self.sids):
             self.e.submit_device(sid, *self.pools[k][2][int(idx[k])])
 
-    def queue_host(self):
-        """The next picture of every stream from host memory, in one call."""
+    def queue_host(self, wait=True):
+        """The next picture of every stream from host memory, in one call
+        (wait=False: the copies run while the caller goes on)."""
         idx = self._advance()
         y = self.base + idx * self.fbytes
-        self.e.submit_batch(self.sids, y, y + self.ny, y + self.ny + self.ny // 4)
+        self.e.submit_batch(self.sids, y, y + self.ny, y + self.ny + self.ny // 4, wait=wait)
 
 
 def ours(args, world, rank, local, dist):
@@ -312,7 +319,7 @@ def ours(args, world, rank, local, dist):
         run.queue_device() if i % 2 else run.queue_host()
         eng.step()
         eng.sync()
-        run.retire()
+        run.retire(run.queued - 1)
 
     # ---- value: device-resident pictures, L2 flushed, the step's two
     # kernels (encode, bitstream) timed with CUDA events on its stream
@@ -330,7 +337,7 @@ def ours(args, world, rank, local, dist):
             bits_ms.append(eng.last_bits_ms())
             eng.sync()
             bits_bytes.append(eng.step_bits()[0])
-            run.retire()
+            run.retire(run.queued - 1)
     torch.cuda.synchronize()
     total_ms = float(sum(kernel_ms) + sum(bits_ms))
     if dist:
@@ -340,39 +347,41 @@ def ours(args, world, rank, local, dist):
     value = mb_per_step * args.steps * world / (total_ms * 1e-3)
 
     # ---- e2e: host pictures in, bitstreams out, through the public API.
-    # Step k is issued, then the host waits for step k-1 and moves its
-    # pictures' bytes out of the host arena while step k runs (the engine
-    # alternates two streams).
+    # Step k is issued, the copies of step k+1's pictures start on the
+    # engine's copy threads, and the host waits for step k-1 and moves its
+    # bitstreams out of the host arena meanwhile (the engine alternates two
+    # streams, so step k runs on the device throughout).
     out = np.empty(64 << 20, np.uint8)
     lat, issued = [], []
     h2d = d2h = 0
 
-    def consume():
+    def consume(k):
         nonlocal d2h
-        pics, span = eng.step_pictures()
+        pics, span = eng.step_pictures(len(streams) + 8)
         assert pics.size == len(streams) and (pics["status"] == 0).all()
         out[:span.size] = span
         d2h += int(pics["bytes"].sum())
+        run.retire(first + k)
+        lat.append((time.perf_counter() - issued[k]) * 1e3)
 
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    first = run.queued
+    run.queue_host(wait=False)
     for it in range(args.steps):
         issued.append(time.perf_counter())
-        run.queue_host()
         eng.step()
         b_in, b_out = eng.last_copy_bytes()
         h2d, d2h = h2d + b_in, d2h + b_out
+        if it + 1 < args.steps:
+            run.queue_host(wait=False)
         if it > 0:
             eng.wait_previous()
-            consume()
-            run.retire()
-            lat.append((time.perf_counter() - issued[it - 1]) * 1e3)
+            consume(it - 1)
     eng.sync()
-    consume()
-    run.retire()
-    lat.append((time.perf_counter() - issued[-1]) * 1e3)
+    consume(args.steps - 1)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     if dist:
@@ -439,7 +448,7 @@ def ours(args, world, rank, local, dist):
                      "traffic": (tr * mb_per_step) if tr else None},
         "sad_roofline": {"achieved": sad_rate, "peak": peak_sad, "unit": "absdiff/s", "frac": sad_rate / peak_sad,
                          "peak_source": "project microbenchmark of the search's SAD step"},
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": 5 * args.steps,   # encode + codes, layout, pack, copy
         "clocks": clk.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:

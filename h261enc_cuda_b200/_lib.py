@@ -78,6 +78,11 @@ class FrameResult(Structure):
                 ("bits", c_void_p), ("bits_bytes", c_int32), ("bits_status", c_int32)]
 
 
+class StepTiming(Structure):
+    _fields_ = [("step", c_int64), ("upload_ms", c_float), ("wait_ms", c_float), ("encode_ms", c_float),
+                ("bitstream_ms", c_float), ("total_ms", c_float), ("reserved", c_float)]
+
+
 class SynthParams(Structure):
     _fields_ = [("width", c_int32), ("height", c_int32), ("kind", c_int32), ("seed", c_uint64),
                 ("n_objects", c_int32), ("obj_min", c_int32), ("obj_max", c_int32),
@@ -119,6 +124,8 @@ def core() -> ctypes.CDLL:
                                             POINTER(POINTER(c_uint8)), POINTER(POINTER(c_uint8))]
         lib.h261b_engine_submit_batch.argtypes = [c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
                                                   c_void_p]
+        lib.h261b_engine_submit_batch_async.argtypes = lib.h261b_engine_submit_batch.argtypes
+        lib.h261b_engine_step_timing.argtypes = [c_void_p, POINTER(StepTiming)]
         lib.h261b_engine_last_bits_ms.argtypes = [c_void_p, POINTER(c_float)]
         lib.h261b_engine_step_pictures.argtypes = [c_void_p, c_int32, c_void_p, POINTER(c_int32),
                                                    POINTER(c_void_p), POINTER(ctypes.c_int64)]

@@ -222,6 +222,10 @@ struct h261b_engine_s {
     cudaEvent_t step_done[2] = { nullptr, nullptr };
     cudaEvent_t k_start[2] = { nullptr, nullptr }, k_end[2] = { nullptr, nullptr };
     cudaEvent_t b_end[2] = { nullptr, nullptr };   /* after the bitstream kernel */
+    /* timing of each phase of a step: begin, uploads done, kernels may
+     * start (the previous step's encode is done), results downloaded */
+    cudaEvent_t t_begin[2] = { nullptr, nullptr }, t_h2d[2] = { nullptr, nullptr };
+    cudaEvent_t t_ready[2] = { nullptr, nullptr }, t_end[2] = { nullptr, nullptr };
     bool step_bits_ran[2] = { false, false };
     bool in_flight[2] = { false, false };
     int64_t step_mbs[2] = { 0, 0 };   /* MB records of the step in each arena */
@@ -333,7 +337,9 @@ extern "C" int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engin
              cudaEventCreateWithFlags(&e->kernel_done[p], cudaEventDisableTiming) == cudaSuccess &&
              cudaEventCreateWithFlags(&e->step_done[p], cudaEventDisableTiming) == cudaSuccess &&
              cudaEventCreate(&e->k_start[p]) == cudaSuccess && cudaEventCreate(&e->k_end[p]) == cudaSuccess &&
-             cudaEventCreate(&e->b_end[p]) == cudaSuccess;
+             cudaEventCreate(&e->b_end[p]) == cudaSuccess && cudaEventCreate(&e->t_begin[p]) == cudaSuccess &&
+             cudaEventCreate(&e->t_h2d[p]) == cudaSuccess && cudaEventCreate(&e->t_ready[p]) == cudaSuccess &&
+             cudaEventCreate(&e->t_end[p]) == cudaSuccess;
     }
     if (!ok) {
         set_error("h261b_engine_create: device setup failed: %s", cudaGetErrorString(cudaGetLastError()));
@@ -361,6 +367,8 @@ extern "C" int h261b_engine_destroy(h261b_engine_t *e)
     if (!e)
         return H261B_OK;
     cudaSetDevice(e->cfg.device);
+    if (e->copier)
+        e->copier->join();
     for (int p = 0; p < 2; p++)
         if (e->stream[p])
             cudaStreamSynchronize(e->stream[p]);
@@ -375,6 +383,10 @@ extern "C" int h261b_engine_destroy(h261b_engine_t *e)
         cudaEventDestroy(e->k_start[p]);
         cudaEventDestroy(e->k_end[p]);
         cudaEventDestroy(e->b_end[p]);
+        cudaEventDestroy(e->t_begin[p]);
+        cudaEventDestroy(e->t_h2d[p]);
+        cudaEventDestroy(e->t_ready[p]);
+        cudaEventDestroy(e->t_end[p]);
         if (e->stream[p])
             cudaStreamDestroy(e->stream[p]);
     }
@@ -507,6 +519,7 @@ static int ensure_capacity(h261b_engine_t *e, int p)
     const size_t desc = sizeof(h261b_step_dev_t) + align_up((size_t)n * sizeof(h261b_session_dev_t), 256) +
                         (size_t)n * H261B_MAX_MB_PER_SESSION * sizeof(uint32_t);
     if (up > e->upload[p].cap || res > e->results[p].cap || desc > e->desc[p].cap) {
+        e->copier->join();   /* copies in flight write into the upload arena */
         H261B_CUDA_TRY(cudaStreamSynchronize(e->stream[p]));
         int rc;
         const size_t keep = e->upload_checked ? e->upload_used : 0;
@@ -610,8 +623,8 @@ extern "C" int h261b_engine_inputs(h261b_engine_t *e, int32_t n, const int32_t *
     return H261B_OK;
 }
 
-extern "C" int h261b_engine_submit_batch(h261b_engine_t *e, int32_t n, const int32_t *ids, const uint8_t *const *y,
-                                         const uint8_t *const *cb, const uint8_t *const *cr, const int32_t *quants)
+static int submit_batch(h261b_engine_t *e, int32_t n, const int32_t *ids, const uint8_t *const *y,
+                        const uint8_t *const *cb, const uint8_t *const *cr, const int32_t *quants, bool async)
 {
     clear_error();
     if (!e || n < 0 || (n > 0 && (!ids || !y || !cb || !cr))) {
@@ -623,6 +636,7 @@ extern "C" int h261b_engine_submit_batch(h261b_engine_t *e, int32_t n, const int
             set_error("h261b_engine_submit_batch: NULL plane for picture %d", i);
             return H261B_ERR_ARG;
         }
+    e->copier->join();   /* one batch in flight at a time */
     std::vector<int64_t> offs((size_t)n * 3);
     uint8_t *staging = nullptr;
     int rc = h261b_engine_inputs(e, n, ids, quants, &staging, offs.data());
@@ -637,8 +651,24 @@ extern "C" int h261b_engine_submit_batch(h261b_engine_t *e, int32_t n, const int
         jobs.push_back({ staging + offs[3 * i + 1], cb[i], nc });
         jobs.push_back({ staging + offs[3 * i + 2], cr[i], nc });
     }
-    e->copier->run(jobs);
+    if (async)
+        e->copier->start(jobs);
+    else
+        e->copier->run(jobs);
     return H261B_OK;
+}
+
+extern "C" int h261b_engine_submit_batch(h261b_engine_t *e, int32_t n, const int32_t *ids, const uint8_t *const *y,
+                                         const uint8_t *const *cb, const uint8_t *const *cr, const int32_t *quants)
+{
+    return submit_batch(e, n, ids, y, cb, cr, quants, false);
+}
+
+extern "C" int h261b_engine_submit_batch_async(h261b_engine_t *e, int32_t n, const int32_t *ids,
+                                               const uint8_t *const *y, const uint8_t *const *cb,
+                                               const uint8_t *const *cr, const int32_t *quants)
+{
+    return submit_batch(e, n, ids, y, cb, cr, quants, true);
 }
 
 extern "C" int h261b_engine_step_records(h261b_engine_t *e, const h261b_mb_result_t **records, int64_t *count,
@@ -824,13 +854,17 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
     }
     cudaStream_t st = e->stream[p];
     const size_t desc_bytes = work_off + (size_t)n_work * sizeof(uint32_t);
+    e->copier->join();   /* pictures of h261b_engine_submit_batch_async */
+    H261B_CUDA_TRY(cudaEventRecord(e->t_begin[p], st));
     H261B_CUDA_TRY(cudaMemcpyAsync(dm.dev, dm.host, desc_bytes, cudaMemcpyHostToDevice, st));
     if (e->upload_checked && e->upload_used)
         H261B_CUDA_TRY(cudaMemcpyAsync(um.dev, um.host, e->upload_used, cudaMemcpyHostToDevice, st));
     H261B_CUDA_TRY(cudaEventRecord(e->h2d_done[p], st));
+    H261B_CUDA_TRY(cudaEventRecord(e->t_h2d[p], st));
     /* the previous step's reconstructions are this step's references */
     if (id > 0)
         H261B_CUDA_TRY(cudaStreamWaitEvent(st, e->kernel_done[p ^ 1], 0));
+    H261B_CUDA_TRY(cudaEventRecord(e->t_ready[p], st));
 
     int warps, ctas;
     const int tuning = next_launch_shape(e, &warps, &ctas);
@@ -863,6 +897,7 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
     H261B_CUDA_TRY(cudaMemcpyAsync(rm.host, rm.dev, d2h, cudaMemcpyDeviceToHost, st));
     e->last_h2d = (int64_t)desc_bytes + (e->upload_checked ? (int64_t)e->upload_used : 0);
     e->last_d2h = (int64_t)d2h;
+    H261B_CUDA_TRY(cudaEventRecord(e->t_end[p], st));
     H261B_CUDA_TRY(cudaEventRecord(e->step_done[p], st));
     e->in_flight[p] = true;
     e->step_mbs[p] = total_mb;
@@ -1076,6 +1111,32 @@ extern "C" int h261b_engine_last_bits_ms(h261b_engine_t *e, float *ms)
         return H261B_OK;
     H261B_CUDA_TRY(cudaEventSynchronize(e->b_end[p]));
     H261B_CUDA_TRY(cudaEventElapsedTime(ms, e->k_end[p], e->b_end[p]));
+    return H261B_OK;
+}
+
+extern "C" int h261b_engine_step_timing(h261b_engine_t *e, h261b_step_timing_t *t)
+{
+    clear_error();
+    if (!e || !t)
+        return H261B_ERR_ARG;
+    if (e->done_step < 0) {
+        set_error("h261b_engine_step_timing: no step has completed");
+        return H261B_ERR_STATE;
+    }
+    const int p = (int)(e->done_step & 1);
+    float a = 0, b = 0, c = 0, d = 0, f = 0;
+    H261B_CUDA_TRY(cudaEventElapsedTime(&a, e->t_begin[p], e->t_h2d[p]));
+    H261B_CUDA_TRY(cudaEventElapsedTime(&b, e->t_h2d[p], e->t_ready[p]));
+    H261B_CUDA_TRY(cudaEventElapsedTime(&c, e->k_start[p], e->k_end[p]));
+    if (e->step_bits_ran[p])
+        H261B_CUDA_TRY(cudaEventElapsedTime(&d, e->k_end[p], e->b_end[p]));
+    H261B_CUDA_TRY(cudaEventElapsedTime(&f, e->t_begin[p], e->t_end[p]));
+    t->step = e->done_step;
+    t->upload_ms = a;
+    t->wait_ms = b;
+    t->encode_ms = c;
+    t->bitstream_ms = d;
+    t->total_ms = f;
     return H261B_OK;
 }
 

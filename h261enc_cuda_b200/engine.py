@@ -115,24 +115,25 @@ class Engine:
         arena = np.ctypeslib.as_array((ctypes.c_uint8 * size).from_address(base.value))
         return arena, offs
 
-    def submit_batch(self, sids, y_ptrs, cb_ptrs, cr_ptrs, quants=None) -> None:
+    def submit_batch(self, sids, y_ptrs, cb_ptrs, cr_ptrs, quants=None, wait: bool = True) -> None:
         """Queue one host picture for each of ``sids``: plane addresses as
         uint64 arrays (packed planes, e.g. ``frame.ctypes.data`` and the
         offsets of Cb and Cr in it).  The engine's copy threads move the
-        pictures into the staging arena before the call returns."""
+        pictures into the staging arena; with ``wait=False`` the call
+        returns once they have started and the next ``step()`` waits for
+        them (the source memory must stay unchanged until then)."""
         sids = np.ascontiguousarray(sids, np.int32)
         ptrs = [np.ascontiguousarray(a, np.uint64) for a in (y_ptrs, cb_ptrs, cr_ptrs)]
         q = None if quants is None else np.ascontiguousarray(quants, np.int32)
-        check(_lib.core().h261b_engine_submit_batch(self._h, sids.size, sids.ctypes.data, ptrs[0].ctypes.data,
-                                                    ptrs[1].ctypes.data, ptrs[2].ctypes.data,
-                                                    None if q is None else q.ctypes.data),
-              "h261b_engine_submit_batch")
+        fn = _lib.core().h261b_engine_submit_batch if wait else _lib.core().h261b_engine_submit_batch_async
+        check(fn(self._h, sids.size, sids.ctypes.data, ptrs[0].ctypes.data, ptrs[1].ctypes.data,
+                 ptrs[2].ctypes.data, None if q is None else q.ctypes.data), "h261b_engine_submit_batch")
 
-    def submit_frames(self, sids, frames, quants=None) -> None:
+    def submit_frames(self, sids, frames, quants=None, wait: bool = True) -> None:
         """``submit_batch`` for packed frames (uint8 arrays of W*H*3/2)."""
         y = np.array([f.ctypes.data for f in frames], np.uint64)
         ny = np.array([self._dims[int(s)][0] * self._dims[int(s)][1] for s in sids], np.uint64)
-        self.submit_batch(sids, y, y + ny, y + ny + ny // 4, quants)
+        self.submit_batch(sids, y, y + ny, y + ny + ny // 4, quants, wait=wait)
 
     def step_records(self):
         """(step number, MB records of every session that step encoded) for
@@ -190,6 +191,13 @@ class Engine:
         span = (np.ctypeslib.as_array((ctypes.c_uint8 * used.value).from_address(base.value))
                 if used.value else np.empty(0, np.uint8))
         return out[:min(n.value, cap)], span
+
+    def step_timing(self) -> dict:
+        """Device timeline of the latest completed step, in milliseconds."""
+        t = _lib.StepTiming()
+        check(_lib.core().h261b_engine_step_timing(self._h, ctypes.byref(t)), "h261b_engine_step_timing")
+        return {"step": t.step, "upload": t.upload_ms, "wait": t.wait_ms, "encode": t.encode_ms,
+                "bitstream": t.bitstream_ms, "total": t.total_ms}
 
     def step_bits(self):
         """(bytes, pictures) of bitstream the latest completed step wrote."""

@@ -122,6 +122,14 @@ int h261b_engine_inputs(h261b_engine_t *e, int32_t n, const int32_t *ids, const 
 int h261b_engine_submit_batch(h261b_engine_t *e, int32_t n, const int32_t *ids, const uint8_t *const *y,
                               const uint8_t *const *cb, const uint8_t *const *cr, const int32_t *quants);
 
+/* h261b_engine_submit_batch that returns as soon as the copies have started:
+ * the engine's copy threads move the pictures while the caller does other
+ * work (reading the previous step, for one); the next h261b_engine_step()
+ * waits for them.  The source planes must stay unchanged until that step
+ * has been issued. */
+int h261b_engine_submit_batch_async(h261b_engine_t *e, int32_t n, const int32_t *ids, const uint8_t *const *y,
+                                    const uint8_t *const *cb, const uint8_t *const *cr, const int32_t *quants);
+
 /* Queue a picture that is already in device memory (packed planes, pitch W
  * and W/2; Y 16-byte and Cb/Cr 8-byte aligned).  It must stay unchanged
  * until the step that reads it has completed. */
@@ -210,6 +218,16 @@ int h261b_session_recon(h261b_engine_t *e, int32_t session_id, uint8_t *y, uint8
 /* Expand one result into the reference's h261_macroblock_t array (what the
  * reference's GOB / macroblock writers read); mbs[] gets num_mb entries. */
 int h261b_result_to_abi(const h261b_frame_result_t *r, int32_t width, h261_macroblock_t *mbs);
+
+/* Device timeline of the latest completed step (CUDA events on its
+ * stream): uploads, waiting for the previous step's encode kernel, the
+ * encode kernel, the bitstream kernels, and begin to end. */
+typedef struct {
+    int64_t step;
+    float upload_ms, wait_ms, encode_ms, bitstream_ms, total_ms;
+    float reserved;
+} h261b_step_timing_t;
+int h261b_engine_step_timing(h261b_engine_t *e, h261b_step_timing_t *t);
 
 /* Device time of the last step's encode kernel, and of its bitstream
  * kernel (0 without bitstream sessions), in milliseconds (CUDA events). */

@@ -1,7 +1,8 @@
 """The engine's pipelined use: steps issued back to back on its two streams,
 the host reading step k-1 while step k runs, streams ending and new sessions
-taking their place without a drain, and the three ways of queueing host
-pictures (one copy per call, the batched copy, writing in place).  Every
+taking their place without a drain, and the ways of queueing host pictures
+(one copy per call, the batched copy, writing in place, the batched copy
+left running until the next step).  Every
 picture must still be bit-exact to the oracle."""
 import numpy as np
 import pytest
@@ -46,6 +47,8 @@ def _queue(e, live, mode):
             e.submit_frame(s, f)
     elif mode == 1:
         e.submit_frames(sids, frames)
+    elif mode == 3:
+        e.submit_frames(sids, frames, wait=False)   # copies finish inside the next step()
     else:
         arena, offs = e.inputs(sids)
         for inst, f, o in zip(live, frames, offs):
@@ -78,7 +81,7 @@ def test_pipelined_steps_with_turnover_match_oracle(gpu):
         prev, closing, step = None, [], 0
         while live or prev:
             if live:
-                _queue(e, live, step % 3)
+                _queue(e, live, step % 4)
                 assert e.step() == len(live)
             cur = list(live)
             # streams whose last picture is now queued make room for the next
