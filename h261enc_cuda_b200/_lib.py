@@ -69,7 +69,8 @@ class EngineConfig(Structure):
 
 class SessionConfig(Structure):
     _fields_ = [("width", c_int32), ("height", c_int32), ("quant", c_int32),
-                ("intra_period", c_int32), ("denoise", c_int32), ("bitstream", c_int32)]
+                ("intra_period", c_int32), ("denoise", c_int32), ("bitstream", c_int32),
+                ("rate_control", c_int32), ("bitrate", c_int32)]
 
 
 class FrameResult(Structure):
@@ -130,6 +131,8 @@ def core() -> ctypes.CDLL:
         lib.h261b_engine_step_pictures.argtypes = [c_void_p, c_int32, c_void_p, POINTER(c_int32),
                                                    POINTER(c_void_p), POINTER(ctypes.c_int64)]
         lib.h261b_engine_step_bits.argtypes = [c_void_p, POINTER(ctypes.c_int64), POINTER(c_int32)]
+        lib.h261b_session_config_bytes.argtypes = [POINTER(SessionConfig)]
+        lib.h261b_session_config_bytes.restype = c_int64
         lib.h261b_session_bits_bytes.argtypes = [c_int32, c_int32]
         lib.h261b_session_bits_bytes.restype = c_int64
         lib.h261b_engine_last_copy_bytes.argtypes = [c_void_p, POINTER(ctypes.c_int64), POINTER(ctypes.c_int64)]

@@ -37,6 +37,7 @@
 #include <cstring>
 
 #include "h261b_device.h"
+#include "ratectrl_dev.h"
 #include "vlc_tables.h"
 
 namespace h261b {
@@ -332,7 +333,7 @@ __global__ void __launch_bounds__(VLC_THREADS) layout_kernel(const h261b_session
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const bool cif = S.mbw == 22;
     const int ngob = cif ? 12 : 3, nmb = S.mbw * S.mbh;
-    const int gq = S.quant;
+    const int gq = S.rc ? S.rc->picture_quant : S.quant;
     const h261b_mb_info_t *info = S.info_out;
     if (tid == 0)
         bad = 0;
@@ -431,6 +432,9 @@ __global__ void __launch_bounds__(VLC_THREADS) layout_kernel(const h261b_session
     if (tid == 0) {
         S.vlc_total[0] = (int32_t)total;
         S.vlc_total[1] = status != 0 ? status : (any_oob ? H261B_BITS_MISMATCH : 0);
+        /* the rate control learns the picture's size */
+        if (S.rc && S.vlc_total[1] == 0)
+            rc_update(*S.rc, S.frame_type, (int32_t)((total + 7) >> 3));
     }
 }
 
@@ -548,7 +552,7 @@ __global__ void __launch_bounds__(VLC_THREADS) copy_kernel(const h261b_session_d
                 o = (int)a;
         }
         off = o;
-        *S.pic_out = h261b_pic_info_t{ st == 0 ? bytes : 0, o, st, S.quant };
+        *S.pic_out = h261b_pic_info_t{ st == 0 ? bytes : 0, o, st, S.rc ? S.rc->picture_quant : S.quant };
     }
     __syncthreads();
     if (off >= 0) {
@@ -586,7 +590,7 @@ extern "C" int64_t h261b_bits_slot_bytes(int32_t w, int32_t h) { return h261b_bi
 
 extern "C" int h261b_launch_bitstream(h261b_session_dev_t *sessions_dev, int32_t n_sessions, const uint32_t *work_dev,
                                       int32_t n_work, h261b_step_dev_t *step, uint8_t *host_arena_dev,
-                                      int64_t host_cap, int32_t sm_count, void *stream)
+                                      int64_t host_cap, int32_t sm_count, void *stream, void *layout_done_event)
 {
     if (n_work <= 0 || n_sessions <= 0)
         return 0;
@@ -594,6 +598,12 @@ extern "C" int h261b_launch_bitstream(h261b_session_dev_t *sessions_dev, int32_t
     cudaStream_t st = (cudaStream_t)stream;
     codes_kernel<<<ctas, VLC_THREADS, 0, st>>>(sessions_dev, work_dev, n_work);
     layout_kernel<<<n_sessions, VLC_THREADS, 0, st>>>(sessions_dev);
+    if (layout_done_event) {
+        /* the next step's rate control reads what the layout updated */
+        const cudaError_t err = cudaEventRecord((cudaEvent_t)layout_done_event, st);
+        if (err != cudaSuccess)
+            return (int)err;
+    }
     pack_kernel<<<ctas, VLC_THREADS, 0, st>>>(sessions_dev, work_dev, n_work);
     copy_kernel<<<n_sessions, VLC_THREADS, 0, st>>>(sessions_dev, step, host_arena_dev, host_cap);
     return (int)cudaGetLastError();

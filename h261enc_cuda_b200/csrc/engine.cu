@@ -189,6 +189,11 @@ struct Session {
     uint8_t *bits_base[2] = { nullptr, nullptr };
     h261b_bits_layout_t bits_lay = {};
     std::vector<uint8_t> bits_spill;   /* a picture the host arena missed */
+    /* CBR rate control: its state and the mode decisions between the two
+     * encode launches of a step */
+    bool rc = false;
+    h261b_rc_dev_t *rc_dev = nullptr;
+    h261_mb_mode_decision_t *md_dev = nullptr;
     /* queued picture: in the upload arena, or already in device memory */
     bool queued = false;
     size_t src_off = 0;
@@ -222,6 +227,7 @@ struct h261b_engine_s {
     cudaEvent_t step_done[2] = { nullptr, nullptr };
     cudaEvent_t k_start[2] = { nullptr, nullptr }, k_end[2] = { nullptr, nullptr };
     cudaEvent_t b_end[2] = { nullptr, nullptr };   /* after the bitstream kernel */
+    cudaEvent_t layout_done[2] = { nullptr, nullptr };   /* rate control inputs written */
     /* timing of each phase of a step: begin, uploads done, kernels may
      * start (the previous step's encode is done), results downloaded */
     cudaEvent_t t_begin[2] = { nullptr, nullptr }, t_h2d[2] = { nullptr, nullptr };
@@ -283,6 +289,30 @@ extern "C" int64_t h261b_session_bits_bytes(int32_t w, int32_t h)
     return 2 * (int64_t)align_up((size_t)h261b_bits_slot_bytes(w, h), 256);
 }
 
+/* rate-control state and one picture's mode decisions */
+static int64_t rc_bytes(int32_t w, int32_t h)
+{
+    return 256 + (int64_t)align_up((size_t)(w / 16) * (h / 16) * sizeof(h261_mb_mode_decision_t), 256);
+}
+
+static bool session_config_ok(const h261b_session_config_t *c)
+{
+    return c && c->width >= 16 && c->height >= 16 && !(c->width & 15) && !(c->height & 15) &&
+           (c->width / 16) * (c->height / 16) <= H261B_MAX_MB_PER_SESSION && c->quant >= 1 && c->quant <= 31 &&
+           c->intra_period >= 0 && c->denoise >= 0 && (c->bitstream == 0 || c->bitstream == 1) &&
+           (c->rate_control == 0 || (c->rate_control == 1 && c->bitstream == 1 && c->bitrate >= 8));
+}
+
+extern "C" int64_t h261b_session_config_bytes(const h261b_session_config_t *c)
+{
+    if (!session_config_ok(c))
+        return H261B_ERR_ARG;
+    const int64_t bits = c->bitstream ? h261b_session_bits_bytes(c->width, c->height) : 0;
+    if (c->bitstream && bits == 0)
+        return H261B_ERR_ARG;
+    return h261b_session_bytes(c->width, c->height) + bits + (c->rate_control ? rc_bytes(c->width, c->height) : 0);
+}
+
 /* return retired session slots whose last step has completed */
 static void reclaim(h261b_engine_t *e)
 {
@@ -338,6 +368,7 @@ extern "C" int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engin
              cudaEventCreateWithFlags(&e->step_done[p], cudaEventDisableTiming) == cudaSuccess &&
              cudaEventCreate(&e->k_start[p]) == cudaSuccess && cudaEventCreate(&e->k_end[p]) == cudaSuccess &&
              cudaEventCreate(&e->b_end[p]) == cudaSuccess && cudaEventCreate(&e->t_begin[p]) == cudaSuccess &&
+             cudaEventCreateWithFlags(&e->layout_done[p], cudaEventDisableTiming) == cudaSuccess &&
              cudaEventCreate(&e->t_h2d[p]) == cudaSuccess && cudaEventCreate(&e->t_ready[p]) == cudaSuccess &&
              cudaEventCreate(&e->t_end[p]) == cudaSuccess;
     }
@@ -383,6 +414,7 @@ extern "C" int h261b_engine_destroy(h261b_engine_t *e)
         cudaEventDestroy(e->k_start[p]);
         cudaEventDestroy(e->k_end[p]);
         cudaEventDestroy(e->b_end[p]);
+        cudaEventDestroy(e->layout_done[p]);
         cudaEventDestroy(e->t_begin[p]);
         cudaEventDestroy(e->t_h2d[p]);
         cudaEventDestroy(e->t_ready[p]);
@@ -406,10 +438,9 @@ static Session *get_session(h261b_engine_t *e, int32_t id)
 extern "C" int h261b_session_open(h261b_engine_t *e, const h261b_session_config_t *c, int32_t *id)
 {
     clear_error();
-    if (!e || !c || !id || c->width < 16 || c->height < 16 || (c->width & 15) || (c->height & 15) ||
-        (c->width / 16) * (c->height / 16) > H261B_MAX_MB_PER_SESSION || c->quant < 1 || c->quant > 31 ||
-        c->intra_period < 0 || c->denoise < 0 || (c->bitstream != 0 && c->bitstream != 1)) {
-        set_error("h261b_session_open: bad session configuration");
+    if (!e || !id || !session_config_ok(c)) {
+        set_error("h261b_session_open: bad session configuration%s",
+                  c && c->rate_control ? " (rate control needs bitstream = 1 and a bitrate)" : "");
         return H261B_ERR_ARG;
     }
     const int64_t bits_need = c->bitstream ? h261b_session_bits_bytes(c->width, c->height) : 0;
@@ -418,7 +449,7 @@ extern "C" int h261b_session_open(h261b_engine_t *e, const h261b_session_config_
                   c->width, c->height);
         return H261B_ERR_ARG;
     }
-    const int64_t need = h261b_session_bytes(c->width, c->height) + bits_need;
+    const int64_t need = h261b_session_config_bytes(c);
     if (e->cfg.hbm_budget_bytes > 0 && e->session_bytes + need > e->cfg.hbm_budget_bytes) {
         set_error("h261b_session_open: HBM budget %lld exceeded", (long long)e->cfg.hbm_budget_bytes);
         return H261B_ERR_BUDGET;
@@ -462,6 +493,23 @@ extern "C" int h261b_session_open(h261b_engine_t *e, const h261b_session_config_
         s.bits_base[0] = b0;
         s.bits_base[1] = b0 + sb;
     }
+    h261b_rc_dev_t rc0;
+    if (c->rate_control) {
+        uint8_t *r0 = base + h261b_session_bytes(c->width, c->height) + bits_need;
+        s.rc = true;
+        s.rc_dev = (h261b_rc_dev_t *)r0;
+        s.md_dev = (h261_mb_mode_decision_t *)(r0 + 256);
+        /* h261_init_ratectrl(ctx, quant, bitrate, bitrate, CBR)
+         * (src/h261_ratectrl.c:107-127) */
+        memset(&rc0, 0, sizeof(rc0));
+        rc0.current_quant = c->quant;
+        rc0.prediction_cost[0] = rc0.prediction_cost[1] = 100;
+        rc0.prediction_size[0] = rc0.prediction_size[1] = 1;
+        rc0.bitrate = c->bitrate / 8;
+        rc0.vbv_size = c->bitrate / 8;
+        rc0.vbv_fill = rc0.vbv_size;
+        rc0.picture_quant = c->quant;
+    }
     /* the first reference is black like the reference's zeroed frame
      * (h261_main.c:155-157); denoise state starts at zero
      * (gpu_device.cu:495-508).  No step in flight touches this slot (a
@@ -477,6 +525,8 @@ extern "C" int h261b_session_open(h261b_engine_t *e, const h261b_session_config_
     H261B_CUDA_TRY(cudaMemsetAsync(base, 0, 2 * s.lay.bytes, st));
     for (int q = 0; q < 2 && s.bitstream; q++)
         H261B_CUDA_TRY(cudaMemsetAsync(s.bits_base[q] + s.bits_lay.total, 0, 256, st));
+    if (s.rc)
+        H261B_CUDA_TRY(cudaMemcpyAsync(s.rc_dev, &rc0, sizeof(rc0), cudaMemcpyHostToDevice, st));
     H261B_CUDA_TRY(cudaMemcpyAsync(s.dn, &dn0, sizeof(dn0), cudaMemcpyHostToDevice, st));
     s.open = true;
     e->open_count++;
@@ -788,7 +838,7 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
     const size_t pic_base = align_up((size_t)total_mb * sizeof(h261b_mb_info_t), 256);
     const size_t levels_base = align_up(pic_base + n * sizeof(h261b_pic_info_t), 256);
     size_t res_off = levels_base;
-    int32_t n_work = 0, n_bits = 0;
+    int32_t n_work = 0, n_bits = 0, n_rc = 0, rc_begin = 0;
     for (size_t k = 0; k < n; k++) {
         Session &s = e->sessions[(size_t)list[k]];
         if (s.queued_quant > 0)
@@ -849,8 +899,25 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
             d.vlc_total = (int32_t *)(bb + L.total);
             n_bits++;
         }
-        for (int32_t m = 0; m < s.nmb; m++)
-            work[n_work++] = ((uint32_t)k << 12) | (uint32_t)m;
+        if (s.rc) {
+            d.rc = s.rc_dev;
+            d.md_out = s.md_dev;
+            d.md_in = s.md_dev;
+            n_rc++;
+        }
+    }
+    /* work list: the MBs of fixed-QUANT sessions, then those of
+     * rate-controlled ones (the second encode launch takes that tail) */
+    for (int pass = 0; pass < 2; pass++) {
+        if (pass == 1)
+            rc_begin = n_work;
+        for (size_t k = 0; k < n; k++) {
+            const Session &s = e->sessions[(size_t)list[k]];
+            if ((int)s.rc != pass)
+                continue;
+            for (int32_t m = 0; m < s.nmb; m++)
+                work[n_work++] = ((uint32_t)k << 12) | (uint32_t)m;
+        }
     }
     cudaStream_t st = e->stream[p];
     const size_t desc_bytes = work_off + (size_t)n_work * sizeof(uint32_t);
@@ -871,7 +938,19 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
     H261B_CUDA_TRY(cudaEventRecord(e->k_start[p], st));
     const int phases = H261B_PHASE_ME | H261B_PHASE_MD | H261B_PHASE_ENCDEC | (e->cfg.fmad ? 0x100 : 0);
     const h261b_session_dev_t *desc_dev = (const h261b_session_dev_t *)(dm.dev + desc_off);
-    int lr = h261b_launch_step(desc_dev, (const uint32_t *)(dm.dev + work_off), n_work, phases, warps, ctas, st);
+    const uint32_t *work_dev = (const uint32_t *)(dm.dev + work_off);
+    int lr = h261b_launch_step(desc_dev, work_dev, n_work, phases, warps, ctas, st);
+    if (lr == 0 && n_rc) {
+        /* rate-controlled sessions: the picture QUANT from this picture's
+         * costs and the previous picture's size (written by the previous
+         * step's layout kernel), then their encode */
+        if (id > 0)
+            H261B_CUDA_TRY(cudaStreamWaitEvent(st, e->layout_done[p ^ 1], 0));
+        lr = h261b_launch_ratectrl((h261b_session_dev_t *)(dm.dev + desc_off), (int32_t)n, st);
+        if (lr == 0)
+            lr = h261b_launch_step(desc_dev, work_dev + rc_begin, n_work - rc_begin,
+                                   H261B_PHASE_ENCDEC | (e->cfg.fmad ? 0x100 : 0), warps, ctas, st);
+    }
     if (lr != 0) {
         set_error("step launch failed: %s", cudaGetErrorString((cudaError_t)lr));
         return H261B_ERR_CUDA;
@@ -884,7 +963,8 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
             return rc;
         lr = h261b_launch_bitstream((h261b_session_dev_t *)(dm.dev + desc_off), (int32_t)n,
                                     (const uint32_t *)(dm.dev + work_off), n_work, (h261b_step_dev_t *)dm.dev,
-                                    e->bits[p].dev, (int64_t)e->bits[p].cap, e->sm_count, st);
+                                    e->bits[p].dev, (int64_t)e->bits[p].cap, e->sm_count, st,
+                                    (void *)e->layout_done[p]);
         if (lr != 0) {
             set_error("bitstream launch failed: %s", cudaGetErrorString((cudaError_t)lr));
             return H261B_ERR_CUDA;
@@ -987,6 +1067,7 @@ extern "C" int h261b_session_result(h261b_engine_t *e, int32_t id, h261b_frame_r
     out->bits_status = 0;
     if (best->has_bits) {
         const h261b_pic_info_t &pi = *(const h261b_pic_info_t *)(rm.host + best->pic_off);
+        out->quant = pi.quant;   /* the rate control's choice for CBR sessions */
         if (pi.status != 0) {
             out->bits_status = H261B_ERR_STATE;
         } else if (pi.host_off >= 0) {

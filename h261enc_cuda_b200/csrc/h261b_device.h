@@ -46,6 +46,21 @@ typedef struct {
                                  the session writes none)                   */
 } h261b_mb_info_t;
 
+/* CBR rate control of one session (src/h261_ratectrl.c h261_ratectrl_t,
+ * 6-bit fixed point), in HBM between pictures */
+typedef struct {
+    int32_t current_quant;
+    int32_t prediction_cost[2];   /* [intra, inter]                         */
+    int32_t prediction_size[2];
+    int32_t bitrate;              /* bytes per second                       */
+    int32_t vbv_size;             /* bytes                                  */
+    int32_t vbv_fill;
+    int32_t current_picture_cost;
+    int32_t picture_quant;        /* QUANT of the picture in flight         */
+    int32_t cost_sum;             /* its summed mode-decision costs         */
+    int32_t reserved[5];
+} h261b_rc_dev_t;
+
 /* per-picture result of the bitstream writer (16 bytes) */
 typedef struct {
     int32_t bytes;            /* picture size in bytes                       */
@@ -101,6 +116,10 @@ typedef struct {
     int32_t *vlc_pos;             /* per MB: bit position in the picture     */
     uint32_t *vlc_plan;           /* per MB: header fields                   */
     int32_t *vlc_total;           /* [0] picture bits, [1] status            */
+    /* CBR sessions: the step's first encode launch runs search and mode
+     * decision (into md_out, costs summed into rc), the rate control picks
+     * the picture QUANT, a second launch encodes (md_in = md_out) */
+    h261b_rc_dev_t *rc;
 } h261b_session_dev_t;
 
 /* coefficient bits of one MB at most: six blocks of an 8-bit DC or a first
@@ -120,6 +139,9 @@ int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const uint32_t *w
                       int32_t n_work, int32_t phases, int32_t warps_per_cta, int32_t max_ctas,
                       void *stream);
 int h261b_set_quant_table(void);
+/* the picture QUANT of every session with rc (one thread per session) */
+int h261b_launch_ratectrl(h261b_session_dev_t *sessions_dev, int32_t n_sessions, void *stream);
+
 /* the bitstream of every work item's session that has bits_out: four
  * launches (coefficient codes and packing over the step's work list,
  * layout and the host copy per session);
@@ -127,7 +149,7 @@ int h261b_set_quant_table(void);
  * memory, host_cap bytes) at an offset drawn from step->host_used */
 int h261b_launch_bitstream(h261b_session_dev_t *sessions_dev, int32_t n_sessions, const uint32_t *work_dev,
                            int32_t n_work, h261b_step_dev_t *step, uint8_t *host_arena_dev, int64_t host_cap,
-                           int32_t sm_count, void *stream);
+                           int32_t sm_count, void *stream, void *layout_done_event);
 /* device bytes per step parity a w x h session's bitstream needs: picture
  * bytes, MB scratch and offsets (0: no bitstream for this size), and where
  * each part starts in that block */

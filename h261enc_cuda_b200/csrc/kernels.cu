@@ -851,6 +851,8 @@ __global__ void __launch_bounds__(256) step_kernel(const h261b_session_dev_t *__
                 me.i_intra_cost = (int32_t)__reduce_add_sync(FULL, lane < 16 ? (uint32_t)v : 0u);
             }
             m = mode_decide(me, S.frame_type);
+            if (lane == 0 && S.rc)
+                atomicAdd(&S.rc->cost_sum, m.cost);   /* the rate control's picture cost */
             if (lane == 0 && S.md_out) {
                 h261_mb_mode_decision_t o;
                 o.i_cost = m.cost;
@@ -873,7 +875,9 @@ __global__ void __launch_bounds__(256) step_kernel(const h261b_session_dev_t *__
             m.flags = m.mvx = m.mvy = m.cost = 0;
         }
 
-        if (want_enc) {
+        /* a rate-controlled session is encoded by a second launch, once its
+         * picture QUANT is known */
+        if (want_enc && !(S.rc && (phases & H261B_PHASE_MD))) {
             const int t = m.type == H261B_MB_TYPE_INTRA ? 0 : 1;
             if (run_n > 0 && (sidx != run_s || t != run_t)) {
                 publish_run(sessions[run_s], run_t, run_n, colsum, lane);
@@ -884,7 +888,7 @@ __global__ void __launch_bounds__(256) step_kernel(const h261b_session_dev_t *__
             }
             run_s = sidx;
             run_t = t;
-            int quant = S.quant;
+            int quant = S.rc ? S.rc->picture_quant : S.quant;
             if (S.md_in && !(phases & H261B_PHASE_MD))
                 quant += S.md_in[mb].i_quantiser_adjust;
             quant = min(31, max(1, quant)); /* gpu_device.cu:625-627 */

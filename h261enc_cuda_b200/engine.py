@@ -65,8 +65,11 @@ class Engine:
 
     # -- sessions
     def open(self, width: int, height: int, quant: int, intra_period: int = 0, denoise: int = 5,
-             bitstream: int = 0) -> int:
-        c = _lib.SessionConfig(width, height, quant, intra_period, denoise, bitstream)
+             bitstream: int = 0, rate_control: int = 0, bitrate: int = 0) -> int:
+        """A new encode session.  rate_control=1: the reference's CBR rate
+        control at `bitrate` bit/s on the device, starting at `quant`
+        (needs bitstream=1)."""
+        c = _lib.SessionConfig(width, height, quant, intra_period, denoise, bitstream, rate_control, bitrate)
         sid = ctypes.c_int32()
         check(_lib.core().h261b_session_open(self._h, ctypes.byref(c), ctypes.byref(sid)), "h261b_session_open")
         self._dims[sid.value] = (width, height)
@@ -249,6 +252,13 @@ class Engine:
             self.destroy()
         except Exception:
             pass
+
+
+def session_config_bytes(width: int, height: int, bitstream: int = 0, rate_control: int = 0, bitrate: int = 0,
+                         quant: int = 8) -> int:
+    """Device bytes (the admission charge) of a session of this configuration."""
+    c = _lib.SessionConfig(width, height, quant, 0, 5, bitstream, rate_control, bitrate)
+    return check(_lib.core().h261b_session_config_bytes(ctypes.byref(c)), "h261b_session_config_bytes")
 
 
 def session_bytes(width: int, height: int) -> int:

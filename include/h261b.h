@@ -82,6 +82,11 @@ typedef struct {
     int32_t bitstream;        /* 1: write each picture's H.261 bitstream on
                                  the device (QCIF and CIF only), the bytes
                                  the reference's writers produce             */
+    int32_t rate_control;     /* 0: fixed QUANT; 1: the reference's CBR rate
+                                 control on the device (needs bitstream = 1;
+                                 `quant` is its starting QUANT, the
+                                 reference uses 10)                          */
+    int32_t bitrate;          /* bit/s for rate_control = 1 (VBV = 1 s)      */
 } h261b_session_config_t;
 
 /* Device bytes one session of this size holds (pictures + state), and the
@@ -89,6 +94,9 @@ typedef struct {
  * size the H.261 syntax has no source format for). */
 int64_t h261b_session_bytes(int32_t width, int32_t height);
 int64_t h261b_session_bits_bytes(int32_t width, int32_t height);
+/* all device bytes a session of this configuration holds (the admission
+ * charge), or a negative status for an invalid configuration */
+int64_t h261b_session_config_bytes(const h261b_session_config_t *cfg);
 
 int h261b_session_open(h261b_engine_t *e, const h261b_session_config_t *cfg, int32_t *session_id);
 int h261b_session_close(h261b_engine_t *e, int32_t session_id);

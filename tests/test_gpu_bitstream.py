@@ -116,3 +116,59 @@ def test_bitstream_refused_for_other_sizes(gpu):
         e.step()
         e.sync()
         assert e.result(sid).bits is None
+
+
+def test_rate_control_on_device_matches_reference_fixture(gpu):
+    """The rate-controlled golden case with the rate control on the device:
+    QUANT per picture, bytes and bitstream as the reference chose them."""
+    path = os.path.join(HERE, "cif_scenes_cbr384k.json")
+    g = json.load(open(path))
+    opt = g["options"]
+    fr = MG.make_input(g["case"])
+    w, h = g["width"], g["height"]
+    with Engine(warps_per_cta=4, levels_to_host=0) as e:
+        sid = e.open(w, h, 10, intra_period=opt["intra"], bitstream=1, rate_control=1, bitrate=opt["bitrate"])
+        for i, want in enumerate(g["per_frame"]):
+            e.submit_frame(sid, fr[i])
+            e.step()
+            e.sync()
+            r = e.result(sid)
+            assert r.quant == want["quant"], f"picture {i}: QUANT {r.quant} != {want['quant']}"
+            assert MG.sha(r.bits) == want["bits"], f"picture {i}: bitstream differs"
+
+
+def test_rate_control_mixed_batch_pipelined_matches_oracle(gpu):
+    """CBR and fixed-QUANT sessions in the same steps, issued back to back:
+    every stream equals the oracle's frame loop with its own settings."""
+    specs = [(352, 288, 0, 256000, 41), (176, 144, 9, 0, 42), (176, 144, 0, 64000, 43), (352, 288, 14, 0, 44),
+             (352, 288, 0, 512000, 45)]
+    n = 8
+    clips = [synth.clip(1 if w == 352 else 2, w, h, seed, n) for (w, h, q, b, seed) in specs]
+    want = [O.encode_stream(c, w, h, quant=q, bitrate=b or 384000, intra_period=5)
+            for c, (w, h, q, b, _) in zip(clips, specs)]
+    got = [b"" for _ in specs]
+    quants = [[] for _ in specs]
+    with Engine(warps_per_cta=4, levels_to_host=0) as e:
+        sids = [e.open(w, h, q or 10, intra_period=5, bitstream=1, rate_control=1 if b else 0, bitrate=b)
+                for (w, h, q, b, _) in specs]
+        for i in range(n + 1):
+            if i < n:
+                e.submit_frames(sids, [c[i] for c in clips])
+                e.step()
+            if i > 0:
+                e.wait_previous() if i < n else e.sync()
+                for k, sid in enumerate(sids):
+                    r = e.result(sid)
+                    got[k] += r.bits
+                    quants[k].append(r.quant)
+    for k in range(len(specs)):
+        assert quants[k] == list(want[k][2]), f"session {k}: QUANTs {quants[k]} vs {list(want[k][2])}"
+        assert got[k] == want[k][0], f"session {k}: bitstream"
+
+
+def test_rate_control_needs_bitstream(gpu):
+    with Engine(warps_per_cta=4) as e:
+        with pytest.raises(RuntimeError):
+            e.open(176, 144, 10, rate_control=1, bitrate=64000)
+        with pytest.raises(RuntimeError):
+            e.open(176, 144, 10, bitstream=1, rate_control=1, bitrate=0)
