@@ -136,6 +136,18 @@ int64_t orc_encode_stream(const uint8_t *yuv, int32_t w, int32_t h, int32_t nfra
                           int32_t me_mode, uint8_t *bits, int64_t bits_cap, int32_t *frame_bytes,
                           int32_t *frame_quant, uint8_t *recon_out);
 
+/* ---- conformance decoder (h261_decoder.c) ---- */
+
+/* parse one picture from bit `pos`: its records (raster MB order), format,
+ * temporal reference; returns the byte-aligned bit position after it or -1 */
+int64_t orc_parse_picture(const uint8_t *bits, int64_t nbytes, int64_t pos, int32_t *w, int32_t *h,
+                          int32_t *tr, h261_macroblock_t *mbs, int32_t mbs_cap);
+/* decode a whole stream (black first reference, pictures of one format) into
+ * packed reconstructions; records optional.  Returns the bytes consumed or
+ * -1 - (index of the picture that failed).  Not reentrant. */
+int64_t orc_decode_stream(const uint8_t *bits, int64_t nbytes, int32_t fmad, uint8_t *recon_out, int32_t max_frames,
+                          h261_macroblock_t *mbs_out, int32_t *frames, int32_t *width, int32_t *height);
+
 #ifdef __cplusplus
 }
 #endif

@@ -70,6 +70,9 @@ def lib() -> ctypes.CDLL:
         L.orc_encode_stream.argtypes = [c_void_p] + [c_int32] * 9 + [c_void_p, ctypes.c_int64, c_void_p,
                                                                         c_void_p, c_void_p]
         L.orc_encode_stream.restype = ctypes.c_int64
+        L.orc_decode_stream.argtypes = [c_void_p, ctypes.c_int64, c_int32, c_void_p, c_int32, c_void_p,
+                                        POINTER(c_int32), POINTER(c_int32), POINTER(c_int32)]
+        L.orc_decode_stream.restype = ctypes.c_int64
         L.orc_rc_init.argtypes = [c_void_p, c_int32, c_int32, c_int32]
         L.orc_rc_picture_quant.argtypes = [c_void_p, c_int32, c_int32, c_int32]
         L.orc_rc_picture_quant.restype = c_int32
@@ -158,6 +161,22 @@ def encode_stream(frames: np.ndarray, width: int, height: int, quant: int = 0, b
     if total < 0:
         raise ValueError(f"orc_encode_stream: status {total}")
     return bits[:total].tobytes(), nb, nq, recon
+
+
+def decode_stream(bits: bytes, max_frames: int = 1024, fmad: int = 1):
+    """The conformance decoder: (reconstructions (n, W*H*3/2), records (n,
+    nmb), width, height) of an H.261 stream of one format."""
+    buf = np.frombuffer(bits, np.uint8)
+    # pictures are stored back to back at their own size
+    recon = np.zeros(max_frames * 352 * 288 * 3 // 2, np.uint8)
+    mbs = np.zeros(max_frames * 396, MB_DTYPE)
+    n, w, h = c_int32(), c_int32(), c_int32()
+    used = lib().orc_decode_stream(_p(buf), buf.size, fmad, _p(recon), max_frames, _p(mbs), ctypes.byref(n),
+                                   ctypes.byref(w), ctypes.byref(h))
+    if used < 0:
+        raise ValueError(f"orc_decode_stream: picture {-1 - used} does not parse")
+    fs, nmb, k = w.value * h.value * 3 // 2, (w.value // 16) * (h.value // 16), n.value
+    return recon[:k * fs].reshape(k, fs).copy(), mbs[:k * nmb].reshape(k, nmb).copy(), w.value, h.value
 
 
 class RateControl:

@@ -172,3 +172,24 @@ def test_rate_control_needs_bitstream(gpu):
             e.open(176, 144, 10, rate_control=1, bitrate=64000)
         with pytest.raises(RuntimeError):
             e.open(176, 144, 10, bitstream=1, rate_control=1, bitrate=0)
+
+
+@pytest.mark.parametrize("preset,w,h,quant,bitrate", [(0, 176, 144, 8, 0), (1, 352, 288, 10, 384000),
+                                                      (3, 176, 144, 2, 0), (2, 352, 288, 20, 0)])
+def test_decoded_bitstream_is_the_device_reconstruction(gpu, preset, w, h, quant, bitrate):
+    """The conformance decoder turns the device's bitstream back into the
+    device's own reconstructions, picture by picture."""
+    fr = synth.clip(preset, w, h, 60 + quant, 7)
+    stream, recs = b"", []
+    with Engine(warps_per_cta=4, levels_to_host=0) as e:
+        sid = e.open(w, h, quant, intra_period=4, bitstream=1, rate_control=1 if bitrate else 0, bitrate=bitrate)
+        for i in range(fr.shape[0]):
+            e.submit_frame(sid, fr[i])
+            e.step()
+            e.sync()
+            stream += e.result(sid).bits
+            recs.append(np.concatenate(e.recon(sid)))
+    drec, dmbs, dw, dh = O.decode_stream(stream)
+    assert (dw, dh) == (w, h) and drec.shape[0] == len(recs)
+    for i in range(len(recs)):
+        assert np.array_equal(drec[i], recs[i]), f"picture {i}: decoded picture differs"
