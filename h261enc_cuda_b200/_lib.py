@@ -70,13 +70,14 @@ class EngineConfig(Structure):
 class SessionConfig(Structure):
     _fields_ = [("width", c_int32), ("height", c_int32), ("quant", c_int32),
                 ("intra_period", c_int32), ("denoise", c_int32), ("bitstream", c_int32),
-                ("rate_control", c_int32), ("bitrate", c_int32)]
+                ("rate_control", c_int32), ("bitrate", c_int32), ("psnr", c_int32)]
 
 
 class FrameResult(Structure):
     _fields_ = [("frame_index", c_int32), ("frame_type", c_int32), ("quant", c_int32),
                 ("num_mb", c_int32), ("mbs", c_void_p), ("levels", POINTER(c_int8)),
-                ("bits", c_void_p), ("bits_bytes", c_int32), ("bits_status", c_int32)]
+                ("bits", c_void_p), ("bits_bytes", c_int32), ("bits_status", c_int32),
+                ("ssd", ctypes.c_uint64 * 3), ("psnr", ctypes.c_double * 3)]
 
 
 class StepTiming(Structure):

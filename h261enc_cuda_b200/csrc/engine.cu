@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -136,6 +137,8 @@ struct Result {
     size_t info_off = 0, level_off = 0;
     size_t pic_off = 0;            /* h261b_pic_info_t of a bitstream session */
     bool has_bits = false;
+    size_t ssd_off = 0;            /* three uint64 squared-error sums        */
+    bool has_ssd = false;
 };
 
 /* pinned host memory the device writes into (mapped) */
@@ -191,6 +194,7 @@ struct Session {
     std::vector<uint8_t> bits_spill;   /* a picture the host arena missed */
     /* CBR rate control: its state and the mode decisions between the two
      * encode launches of a step */
+    bool psnr = false;
     bool rc = false;
     h261b_rc_dev_t *rc_dev = nullptr;
     h261_mb_mode_decision_t *md_dev = nullptr;
@@ -300,6 +304,7 @@ static bool session_config_ok(const h261b_session_config_t *c)
     return c && c->width >= 16 && c->height >= 16 && !(c->width & 15) && !(c->height & 15) &&
            (c->width / 16) * (c->height / 16) <= H261B_MAX_MB_PER_SESSION && c->quant >= 1 && c->quant <= 31 &&
            c->intra_period >= 0 && c->denoise >= 0 && (c->bitstream == 0 || c->bitstream == 1) &&
+           (c->psnr == 0 || c->psnr == 1) &&
            (c->rate_control == 0 || (c->rate_control == 1 && c->bitstream == 1 && c->bitrate >= 8));
 }
 
@@ -479,6 +484,7 @@ extern "C" int h261b_session_open(h261b_engine_t *e, const h261b_session_config_
     s.nmb = s.mbw * s.mbh;
     s.quant = c->quant;
     s.intra_period = c->intra_period;
+    s.psnr = c->psnr != 0;
     s.lay = PictureLayout::of(s.w, s.h);
     s.slot_bytes = (size_t)need;
     uint8_t *base = (uint8_t *)blk;
@@ -561,7 +567,7 @@ static int ensure_capacity(h261b_engine_t *e, int p)
     for (const Session &s : e->sessions)
         if (s.open) {
             up += align_up(s.lay.bytes, 256);
-            res += (size_t)s.nmb * sizeof(h261b_mb_info_t) + sizeof(h261b_pic_info_t) +
+            res += (size_t)s.nmb * sizeof(h261b_mb_info_t) + sizeof(h261b_pic_info_t) + 32 +
                    align_up((size_t)s.nmb * 384, 256);
             n++;
         }
@@ -836,9 +842,10 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
         total_mb += e->sessions[(size_t)sid].nmb;
     size_t info_off = 0;
     const size_t pic_base = align_up((size_t)total_mb * sizeof(h261b_mb_info_t), 256);
-    const size_t levels_base = align_up(pic_base + n * sizeof(h261b_pic_info_t), 256);
+    const size_t ssd_base = align_up(pic_base + n * sizeof(h261b_pic_info_t), 256);
+    const size_t levels_base = align_up(ssd_base + n * 32, 256);
     size_t res_off = levels_base;
-    int32_t n_work = 0, n_bits = 0, n_rc = 0, rc_begin = 0;
+    int32_t n_work = 0, n_bits = 0, n_rc = 0, rc_begin = 0, n_ssd = 0;
     for (size_t k = 0; k < n; k++) {
         Session &s = e->sessions[(size_t)list[k]];
         if (s.queued_quant > 0)
@@ -899,6 +906,12 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
             d.vlc_total = (int32_t *)(bb + L.total);
             n_bits++;
         }
+        r.has_ssd = s.psnr;
+        r.ssd_off = ssd_base + k * 32;
+        if (s.psnr) {
+            d.ssd_out = (unsigned long long *)(rm.dev + r.ssd_off);
+            n_ssd++;
+        }
         if (s.rc) {
             d.rc = s.rc_dev;
             d.md_out = s.md_dev;
@@ -923,6 +936,8 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
     const size_t desc_bytes = work_off + (size_t)n_work * sizeof(uint32_t);
     e->copier->join();   /* pictures of h261b_engine_submit_batch_async */
     H261B_CUDA_TRY(cudaEventRecord(e->t_begin[p], st));
+    if (n_ssd)
+        H261B_CUDA_TRY(cudaMemsetAsync(rm.dev + ssd_base, 0, n * 32, st));
     H261B_CUDA_TRY(cudaMemcpyAsync(dm.dev, dm.host, desc_bytes, cudaMemcpyHostToDevice, st));
     if (e->upload_checked && e->upload_used)
         H261B_CUDA_TRY(cudaMemcpyAsync(um.dev, um.host, e->upload_used, cudaMemcpyHostToDevice, st));
@@ -1065,6 +1080,19 @@ extern "C" int h261b_session_result(h261b_engine_t *e, int32_t id, h261b_frame_r
     out->bits = nullptr;
     out->bits_bytes = 0;
     out->bits_status = 0;
+    for (int c = 0; c < 3; c++) {
+        out->ssd[c] = 0;
+        out->psnr[c] = 0.0;
+    }
+    if (best->has_ssd) {
+        const uint64_t *ssd = (const uint64_t *)(rm.host + best->ssd_off);
+        for (int c = 0; c < 3; c++) {
+            /* h261_main.c:79-86 */
+            const double pels = c == 0 ? (double)s->w * s->h : (double)(s->w / 2) * (s->h / 2);
+            out->ssd[c] = ssd[c];
+            out->psnr[c] = ssd[c] == 0 ? 100.0 : 10 * log10(255.0 * 255.0 * pels / (double)ssd[c]);
+        }
+    }
     if (best->has_bits) {
         const h261b_pic_info_t &pi = *(const h261b_pic_info_t *)(rm.host + best->pic_off);
         out->quant = pi.quant;   /* the rate control's choice for CBR sessions */

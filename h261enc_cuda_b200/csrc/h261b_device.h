@@ -120,6 +120,9 @@ typedef struct {
      * decision (into md_out, costs summed into rc), the rate control picks
      * the picture QUANT, a second launch encodes (md_in = md_out) */
     h261b_rc_dev_t *rc;
+    /* sums of squared errors of the picture's Y, Cb, Cr reconstruction
+     * (sessions that measure PSNR), zeroed before the step */
+    unsigned long long *ssd_out;
 } h261b_session_dev_t;
 
 /* coefficient bits of one MB at most: six blocks of an 8-bit DC or a first

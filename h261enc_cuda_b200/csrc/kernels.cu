@@ -487,7 +487,7 @@ __device__ __forceinline__ int hfilt(uint2 v, int c)
 template <int FMAD>
 __device__ __forceinline__ uint32_t encdec_pass(float (*tb)[72], const StageBuf &s, const h261b_session_dev_t &S,
                                                 int mb, int mbx, int mby, const MbDecision &m, int quant,
-                                                bool luma_pass, int lane, int32_t colsum[8])
+                                                bool luma_pass, int lane, int32_t colsum[8], uint32_t &ssd)
 {
     const bool active = luma_pass || lane < 16;
     const int slot = lane >> 3, r = lane & 7;
@@ -713,6 +713,20 @@ __device__ __forceinline__ uint32_t encdec_pass(float (*tb)[72], const StageBuf 
         else
             dst = ((b == 4) ? S.rec_cb : S.rec_cr) + (size_t)(mby * 8 + r) * S.pitch_c + mbx * 8;
         *reinterpret_cast<uint2 *>(dst) = make_uint2(lo, hi);
+        if (S.ssd_out) {
+            /* squared error of this row against the source, for the
+             * picture's PSNR (h261_main.c:38-91) */
+            const uint2 cw = luma_pass ? *reinterpret_cast<const uint2 *>(&s.cur[(by8 + r) * 4 + (bx8 >> 2)])
+                                       : *reinterpret_cast<const uint2 *>(&s.curc[b - 4][2 * r]);
+            const uint2 rw = make_uint2(lo, hi);
+            uint32_t e = 0;
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const int d = byte8(cw, i) - byte8(rw, i);
+                e += (uint32_t)(d * d);
+            }
+            ssd = e;
+        }
     }
     __syncwarp();
     return cbp;
@@ -892,8 +906,19 @@ __global__ void __launch_bounds__(256) step_kernel(const h261b_session_dev_t *__
             if (S.md_in && !(phases & H261B_PHASE_MD))
                 quant += S.md_in[mb].i_quantiser_adjust;
             quant = min(31, max(1, quant)); /* gpu_device.cu:625-627 */
-            uint32_t cbp = encdec_pass<FMAD>(sm.t, b, S, mb, mbx, mby, m, quant, true, lane, colsum);
-            cbp |= encdec_pass<FMAD>(sm.t, b, S, mb, mbx, mby, m, quant, false, lane, colsum);
+            uint32_t ssd_l = 0, ssd_c = 0;
+            uint32_t cbp = encdec_pass<FMAD>(sm.t, b, S, mb, mbx, mby, m, quant, true, lane, colsum, ssd_l);
+            cbp |= encdec_pass<FMAD>(sm.t, b, S, mb, mbx, mby, m, quant, false, lane, colsum, ssd_c);
+            if (S.ssd_out) {
+                const uint32_t ey = __reduce_add_sync(FULL, ssd_l);
+                const uint32_t ecb = __reduce_add_sync(FULL, lane < 8 ? ssd_c : 0u);
+                const uint32_t ecr = __reduce_add_sync(FULL, lane >= 8 && lane < 16 ? ssd_c : 0u);
+                if (lane == 0) {
+                    atomicAdd(&S.ssd_out[0], (unsigned long long)ey);
+                    atomicAdd(&S.ssd_out[1], (unsigned long long)ecb);
+                    atomicAdd(&S.ssd_out[2], (unsigned long long)ecr);
+                }
+            }
             run_n++;
 
             const int flags = m.flags | (cbp ? H261B_MB_COEFF : 0);

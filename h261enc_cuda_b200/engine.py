@@ -24,6 +24,8 @@ class FrameResult:
     levels: np.ndarray     # int8 [num_mb, 6, 64], per block column-major (u * 8 + v); None if not copied
     bits: bytes = None     # the picture's H.261 bytes (sessions opened with bitstream=1)
     bits_status: int = 0
+    psnr: tuple = None     # (Y, Cb, Cr) dB, sessions opened with psnr=1
+    ssd: tuple = None      # the squared errors they come from
 
     def to_abi(self, width: int) -> np.ndarray:
         """The reference's h261_macroblock_t array for this picture."""
@@ -65,11 +67,12 @@ class Engine:
 
     # -- sessions
     def open(self, width: int, height: int, quant: int, intra_period: int = 0, denoise: int = 5,
-             bitstream: int = 0, rate_control: int = 0, bitrate: int = 0) -> int:
+             bitstream: int = 0, rate_control: int = 0, bitrate: int = 0, psnr: int = 0) -> int:
         """A new encode session.  rate_control=1: the reference's CBR rate
         control at `bitrate` bit/s on the device, starting at `quant`
-        (needs bitstream=1)."""
-        c = _lib.SessionConfig(width, height, quant, intra_period, denoise, bitstream, rate_control, bitrate)
+        (needs bitstream=1).  psnr=1: each result carries the picture's
+        PSNR."""
+        c = _lib.SessionConfig(width, height, quant, intra_period, denoise, bitstream, rate_control, bitrate, psnr)
         sid = ctypes.c_int32()
         check(_lib.core().h261b_session_open(self._h, ctypes.byref(c), ctypes.byref(sid)), "h261b_session_open")
         self._dims[sid.value] = (width, height)
@@ -175,7 +178,9 @@ class Engine:
             mbs = mbs.copy()
             lv = None if lv is None else lv.copy()
         bits = ctypes.string_at(r.bits, r.bits_bytes) if r.bits else None
-        return FrameResult(r.frame_index, r.frame_type, r.quant, mbs, lv, bits, r.bits_status)
+        psnr = tuple(r.psnr) if any(r.ssd) or any(r.psnr) else None
+        return FrameResult(r.frame_index, r.frame_type, r.quant, mbs, lv, bits, r.bits_status, psnr,
+                           tuple(r.ssd) if psnr else None)
 
     def last_bits_ms(self) -> float:
         ms = ctypes.c_float()
@@ -257,7 +262,7 @@ class Engine:
 def session_config_bytes(width: int, height: int, bitstream: int = 0, rate_control: int = 0, bitrate: int = 0,
                          quant: int = 8) -> int:
     """Device bytes (the admission charge) of a session of this configuration."""
-    c = _lib.SessionConfig(width, height, quant, 0, 5, bitstream, rate_control, bitrate)
+    c = _lib.SessionConfig(width, height, quant, 0, 5, bitstream, rate_control, bitrate, 0)
     return check(_lib.core().h261b_session_config_bytes(ctypes.byref(c)), "h261b_session_config_bytes")
 
 

@@ -87,6 +87,9 @@ typedef struct {
                                  `quant` is its starting QUANT, the
                                  reference uses 10)                          */
     int32_t bitrate;          /* bit/s for rate_control = 1 (VBV = 1 s)      */
+    int32_t psnr;             /* 1: measure each picture's PSNR (the
+                                 reference's get_frame_psnr, h261_main.c:38-91)
+                                 from squared errors summed on the device    */
 } h261b_session_config_t;
 
 /* Device bytes one session of this size holds (pictures + state), and the
@@ -183,6 +186,9 @@ typedef struct {
     int32_t bits_status;      /* 0, or negative: the picture has no
                                  bitstream (H261B_ERR_STATE: a record the
                                  syntax cannot express)                      */
+    uint64_t ssd[3];          /* psnr = 1: squared error of Y, Cb, Cr         */
+    double psnr[3];           /* psnr = 1: 10 log10(255^2 N / ssd), 100 when
+                                 ssd = 0, as the reference computes it       */
 } h261b_frame_result_t;
 
 /* Results of the latest completed step that encoded this session (pointers

@@ -136,6 +136,10 @@ int64_t orc_encode_stream(const uint8_t *yuv, int32_t w, int32_t h, int32_t nfra
                           int32_t me_mode, uint8_t *bits, int64_t bits_cap, int32_t *frame_bytes,
                           int32_t *frame_quant, uint8_t *recon_out);
 
+/* per-plane squared error and PSNR of a reconstruction (packed planes), as
+ * src/h261_main.c:38-91 computes them */
+void orc_psnr(const uint8_t *orig, const uint8_t *recon, int32_t w, int32_t h, uint64_t ssd[3], double psnr[3]);
+
 /* ---- conformance decoder (h261_decoder.c) ---- */
 
 /* parse one picture from bit `pos`: its records (raster MB order), format,

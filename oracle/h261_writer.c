@@ -22,6 +22,7 @@
  */
 #include "h261_oracle.h"
 
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -464,4 +465,23 @@ int64_t orc_encode_stream(const uint8_t *yuv, int32_t w, int32_t h, int32_t nfra
     free(md);
     free(mbs);
     return total;
+}
+
+/* ------------------------------------------------------------------ PSNR */
+
+/* per-plane PSNR of a reconstruction, as src/h261_main.c:38-91 computes it */
+void orc_psnr(const uint8_t *orig, const uint8_t *recon, int32_t w, int32_t h, uint64_t ssd[3], double psnr[3])
+{
+    const size_t ny = (size_t)w * h, nc = ny / 4;
+    const size_t off[3] = { 0, ny, ny + nc }, n[3] = { ny, nc, nc };
+    for (int c = 0; c < 3; c++) {
+        uint64_t e = 0;
+        for (size_t i = 0; i < n[c]; i++) {
+            const uint32_t d = (uint32_t)orig[off[c] + i] - (uint32_t)recon[off[c] + i];
+            e += (uint64_t)(d * d);
+        }
+        const int32_t px = c == 0 ? w : w / 2, py = c == 0 ? h : h / 2;
+        ssd[c] = e;
+        psnr[c] = e == 0 ? 100.0 : 10 * log10(255.0 * 255.0 * (px * py) / (double)e);
+    }
 }

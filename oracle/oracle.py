@@ -73,6 +73,7 @@ def lib() -> ctypes.CDLL:
         L.orc_decode_stream.argtypes = [c_void_p, ctypes.c_int64, c_int32, c_void_p, c_int32, c_void_p,
                                         POINTER(c_int32), POINTER(c_int32), POINTER(c_int32)]
         L.orc_decode_stream.restype = ctypes.c_int64
+        L.orc_psnr.argtypes = [c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_void_p]
         L.orc_rc_init.argtypes = [c_void_p, c_int32, c_int32, c_int32]
         L.orc_rc_picture_quant.argtypes = [c_void_p, c_int32, c_int32, c_int32]
         L.orc_rc_picture_quant.restype = c_int32
@@ -177,6 +178,16 @@ def decode_stream(bits: bytes, max_frames: int = 1024, fmad: int = 1):
         raise ValueError(f"orc_decode_stream: picture {-1 - used} does not parse")
     fs, nmb, k = w.value * h.value * 3 // 2, (w.value // 16) * (h.value // 16), n.value
     return recon[:k * fs].reshape(k, fs).copy(), mbs[:k * nmb].reshape(k, nmb).copy(), w.value, h.value
+
+
+def psnr(orig: np.ndarray, recon: np.ndarray, width: int, height: int):
+    """((ssd_y, ssd_cb, ssd_cr), (psnr_y, psnr_cb, psnr_cr)) of one picture,
+    the reference's get_frame_psnr."""
+    ssd = np.zeros(3, np.uint64)
+    out = np.zeros(3, np.float64)
+    lib().orc_psnr(_p(np.ascontiguousarray(orig, np.uint8)), _p(np.ascontiguousarray(recon, np.uint8)), width,
+                   height, _p(ssd), _p(out))
+    return tuple(int(x) for x in ssd), tuple(float(x) for x in out)
 
 
 class RateControl:
