@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batch64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=20.0,
+                    help="length of the serving run (--workload serve)")
     return ap.parse_args()
 
 
@@ -462,6 +464,45 @@ def ours(args, world, rank, local, dist):
         dist.destroy_process_group()
 
 
+def serve(args, world, rank, local, dist):
+    """The serving workload: Poisson arrivals at 200 sessions/s, 70 % QCIF /
+    30 % CIF, 30..600 pictures at 30 per second each, QUANT 4..24, admitted
+    under a 40 GB HBM budget; aggregate MB/s and per-picture latency over
+    the run."""
+    import torch
+    from h261enc_cuda_b200 import serving
+    from h261enc_cuda_b200.engine import Engine
+
+    torch.cuda.set_device(local)
+    reqs = serving.poisson_requests(200.0, args.serve_seconds, seed=100 + rank)
+    pool = serving.ClipPool()
+    with Engine(device=local, max_sessions=8192, levels_to_host=0, hbm_budget_bytes=40 << 30) as e:
+        srv = serving.Server(e, pool, fps=30.0)
+        if dist:
+            dist.barrier()
+        with ClockSampler(local) as clk:
+            st = srv.run(reqs, duration=args.serve_seconds)
+    summ = st.summary()
+    value = st.macroblocks / st.duration
+    if dist:
+        t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t)
+        value = float(t.item())
+    if rank == 0:
+        line = {"metric": "served encoded MB/s (Poisson 200 sessions/s, 30 fps each, HBM-budget admission)",
+                "value": value, "unit": "MB/s", "n_gpus": world, "steps": st.steps, "warmup": 0,
+                "ms_per_step": st.duration * 1e3 / max(st.steps, 1), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u8", "data": "synthetic (shared clip pool)",
+                "config": {"workload": "serve", "seconds": args.serve_seconds, "arrival_rate": 200,
+                           "sessions": len(reqs), "hbm_budget_gb": 40},
+                "latency_ms": summ["latency_ms"], "serving": summ, "gpu_launches": 5 * st.steps,
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     world, rank, local, dist = dist_setup(args)
@@ -469,6 +510,9 @@ def main():
         reference_arm(args, world, rank)
         if dist:
             dist.destroy_process_group()
+        return
+    if args.workload == "serve":
+        serve(args, world, rank, local, dist)
         return
     ours(args, world, rank, local, dist)
 

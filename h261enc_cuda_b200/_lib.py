@@ -19,6 +19,7 @@ SYNTH_PATH = os.path.join(LIB_DIR, "libh261b_synth.so")
 
 H261B_OK = 0
 ERRORS = {-1: "ARG", -2: "CUDA", -3: "NOMEM", -4: "BUDGET", -5: "STATE", -6: "NO_DEVICE"}
+ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_BUDGET, ERR_STATE, ERR_NO_DEVICE = -1, -2, -3, -4, -5, -6
 
 FRAME_TYPE_INTRA, FRAME_TYPE_INTER = 0, 1
 MB_TYPE_INTRA, MB_TYPE_INTER = 0, 2
@@ -180,13 +181,17 @@ def synth() -> ctypes.CDLL:
 
 
 class H261Error(RuntimeError):
-    pass
+    """A failed library call; `status` is its H261B_ERR_* code."""
+
+    def __init__(self, message: str, status: int = 0):
+        super().__init__(message)
+        self.status = status
 
 
 def check(rc: int, what: str) -> int:
     if rc < 0:
         msg = core().h261b_last_error().decode(errors="replace")
-        raise H261Error(f"{what} failed ({ERRORS.get(rc, rc)}): {msg}")
+        raise H261Error(f"{what} failed ({ERRORS.get(rc, rc)}): {msg}", rc)
     return rc
 
 

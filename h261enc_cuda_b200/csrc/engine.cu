@@ -217,6 +217,8 @@ struct h261b_engine_s {
     DevicePool pool;
     std::vector<Session> sessions;
     int32_t open_count = 0;
+    size_t sum_upload = 0, sum_results = 0;   /* arena shares of the open sessions */
+    int64_t sum_mb = 0;
     int64_t session_bytes = 0;
 
     Mirror upload[2];          /* queued source pictures                  */
@@ -440,6 +442,14 @@ static Session *get_session(h261b_engine_t *e, int32_t id)
     return &e->sessions[(size_t)id];
 }
 
+/* arena bytes a step takes at most for one session (every open session
+ * may have a picture in it); kept as running sums over the open sessions */
+static size_t upload_share(const Session &s) { return align_up(s.lay.bytes, 256); }
+static size_t results_share(const Session &s)
+{
+    return (size_t)s.nmb * sizeof(h261b_mb_info_t) + sizeof(h261b_pic_info_t) + 32 + align_up((size_t)s.nmb * 384, 256);
+}
+
 extern "C" int h261b_session_open(h261b_engine_t *e, const h261b_session_config_t *c, int32_t *id)
 {
     clear_error();
@@ -536,6 +546,9 @@ extern "C" int h261b_session_open(h261b_engine_t *e, const h261b_session_config_
     H261B_CUDA_TRY(cudaMemcpyAsync(s.dn, &dn0, sizeof(dn0), cudaMemcpyHostToDevice, st));
     s.open = true;
     e->open_count++;
+    e->sum_upload += upload_share(s);
+    e->sum_results += results_share(s);
+    e->sum_mb += s.nmb;
     e->session_bytes += need;
     *id = slot;
     return H261B_OK;
@@ -553,6 +566,9 @@ extern "C" int h261b_session_close(h261b_engine_t *e, int32_t id)
     reclaim(e);
     e->session_bytes -= (int64_t)s->slot_bytes;
     e->open_count--;
+    e->sum_upload -= upload_share(*s);
+    e->sum_results -= results_share(*s);
+    e->sum_mb -= s->nmb;
     *s = Session();
     return H261B_OK;
 }
@@ -562,18 +578,10 @@ extern "C" int h261b_session_close(h261b_engine_t *e, int32_t id)
  * previous step, still readable by the caller) are not touched */
 static int ensure_capacity(h261b_engine_t *e, int p)
 {
-    size_t up = 0, res = 0;
-    int32_t n = 0;
-    for (const Session &s : e->sessions)
-        if (s.open) {
-            up += align_up(s.lay.bytes, 256);
-            res += (size_t)s.nmb * sizeof(h261b_mb_info_t) + sizeof(h261b_pic_info_t) + 32 +
-                   align_up((size_t)s.nmb * 384, 256);
-            n++;
-        }
-    res += 512;   /* alignment of the record, picture and level regions */
-    const size_t desc = sizeof(h261b_step_dev_t) + align_up((size_t)n * sizeof(h261b_session_dev_t), 256) +
-                        (size_t)n * H261B_MAX_MB_PER_SESSION * sizeof(uint32_t);
+    const size_t up = e->sum_upload;
+    const size_t res = e->sum_results + 512;   /* alignment of the record, picture and level regions */
+    const size_t desc = sizeof(h261b_step_dev_t) + align_up((size_t)e->open_count * sizeof(h261b_session_dev_t), 256) +
+                        (size_t)e->sum_mb * sizeof(uint32_t);
     if (up > e->upload[p].cap || res > e->results[p].cap || desc > e->desc[p].cap) {
         e->copier->join();   /* copies in flight write into the upload arena */
         H261B_CUDA_TRY(cudaStreamSynchronize(e->stream[p]));

@@ -1,0 +1,36 @@
+"""Serving on the GPU: sessions arriving over time, admitted under an HBM
+budget and batched continuously; every kept session's bitstream must be the
+one it produces alone (the oracle's frame loop on the same pictures)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from h261enc_cuda_b200 import serving
+from h261enc_cuda_b200.engine import Engine, session_config_bytes
+
+pytestmark = pytest.mark.gpu
+
+
+def test_served_sessions_equal_their_alone_encodes(gpu):
+    reqs = serving.poisson_requests(30, 1.5, seed=11, frames=(4, 14))
+    assert len(reqs) >= 20
+    keep = [r.rid for r in reqs[::4]]
+    # room for about six CIF sessions: later arrivals wait for earlier ones
+    budget = 6 * session_config_bytes(352, 288, bitstream=1)
+    pool = serving.ClipPool(clips_per_size=3, length=10)
+    with Engine(max_sessions=64, levels_to_host=0, hbm_budget_bytes=budget, warps_per_cta=4) as e:
+        srv = serving.Server(e, pool, fps=30.0, keep_bits_for=keep)
+        st = srv.run(reqs, duration=1.5, drain=True)
+    assert st.admitted == len(reqs) and st.pictures == sum(r.frames for r in reqs)
+    assert st.max_session_bytes <= budget
+    assert st.refused_at_least_once > 0
+    for r in reqs:
+        if r.rid not in keep:
+            continue
+        frames = np.stack([pool.frame(r.width, r.height, r.seed, i) for i in range(r.frames)])
+        want = O.encode_stream(frames, r.width, r.height, quant=r.quant)[0]
+        got = srv.bits[r.rid]
+        assert len(got) == r.frames
+        assert b"".join(got) == want, f"request {r.rid}"
+    summ = st.summary()
+    assert summ["latency_ms"]["p50"] is not None and summ["latency_ms"]["p99"] >= summ["latency_ms"]["p50"]
