@@ -495,7 +495,8 @@ def serve(args, world, rank, local, dist):
                 "vs_baseline": None, "dtype": "u8", "data": "synthetic (shared clip pool)",
                 "config": {"workload": "serve", "seconds": args.serve_seconds, "arrival_rate": 200,
                            "sessions": len(reqs), "hbm_budget_gb": 40},
-                "latency_ms": summ["latency_ms"], "serving": summ, "gpu_launches": 5 * st.steps,
+                "latency_ms": summ["latency_ms"], "latency_ms_second_half": summ["latency_ms_second_half"],
+                "serving": summ, "gpu_launches": 5 * st.steps,
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     if dist:

@@ -99,7 +99,9 @@ struct Mirror {
     {
         if (bytes <= cap)
             return H261B_OK;
-        size_t c = align_up(std::max<size_t>(bytes, 1 << 16) * 5 / 4, 4096);
+        /* doubling: a growing session count reallocates (and syncs) only a
+         * few times */
+        size_t c = align_up(std::max<size_t>(std::max<size_t>(bytes, 1 << 16), 2 * cap), 4096);
         uint8_t *nh = nullptr, *nd = nullptr;
         cudaError_t e1 = cudaMallocHost(&nh, c);
         cudaError_t e2 = cudaMalloc(&nd, c);

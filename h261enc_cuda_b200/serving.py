@@ -101,9 +101,11 @@ class ServeStats:
     max_concurrent: int
     max_session_bytes: int
     latencies_ms: np.ndarray = field(repr=False, default=None)
+    released_s: np.ndarray = field(repr=False, default=None)   # each picture's release time
 
     def summary(self) -> dict:
         lat = self.latencies_ms
+        late = lat[self.released_s >= self.duration / 2] if self.released_s is not None else lat[:0]
         return {
             "duration_s": self.duration, "pictures": self.pictures, "mb_per_s": self.macroblocks / self.duration,
             "steps": self.steps, "pictures_per_step": self.pictures / max(self.steps, 1),
@@ -112,6 +114,9 @@ class ServeStats:
             "latency_ms": {"p50": float(np.percentile(lat, 50)) if lat.size else None,
                            "p99": float(np.percentile(lat, 99)) if lat.size else None,
                            "max": float(lat.max()) if lat.size else None},
+            "latency_ms_second_half": {"p50": float(np.percentile(late, 50)) if late.size else None,
+                                       "p99": float(np.percentile(late, 99)) if late.size else None,
+                                       "max": float(late.max()) if late.size else None},
         }
 
 
@@ -138,6 +143,7 @@ class Server:
         due: list = []                       # heap of (release time, session id), one entry per session
         in_step: Dict[int, list] = {}        # step number -> [(session id, release time)]
         lat: List[float] = []
+        rel: List[float] = []
         refused = set()
         st = {"pictures": 0, "mbs": 0, "bytes": 0, "max_bytes": 0}
         steps = admitted = max_live = 0
@@ -163,6 +169,7 @@ class Server:
                 s.done += 1
                 if now <= duration or drain:
                     lat.append((now - release) * 1e3)
+                    rel.append(release)
                     st["pictures"] += 1
                     st["mbs"] += (s.req.width // 16) * (s.req.height // 16)
                 if s.done == s.req.frames:
@@ -240,7 +247,7 @@ class Server:
                 raise RuntimeError("serving did not drain within 600 s of the end")
         el = clock() - t0 if drain else min(clock() - t0, duration)
         return ServeStats(el, st["pictures"], st["mbs"], steps, admitted, len(refused), max_live, st["max_bytes"],
-                          np.asarray(lat, np.float64))
+                          np.asarray(lat, np.float64), np.asarray(rel, np.float64))
 
     def _bytes(self, r: Request) -> int:
         from .engine import session_config_bytes
