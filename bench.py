@@ -46,6 +46,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 CLIP_LEN = 24
+METRIC = "encoded MB/s (batched 64 mixed QCIF/CIF streams to H.261 bitstreams, bit-exact to the reference)"
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "step_kernel_batch64.md")
@@ -160,15 +161,9 @@ def ncu_traffic_per_mb():
 
 
 def dist_setup(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        import datetime
-        dist.init_process_group("nccl" if args.impl == "ours" else "gloo",
-                                timeout=datetime.timedelta(seconds=120))
+    from h261enc_cuda_b200 import shard
+    world, rank, local = shard.rank_info()
+    dist = shard.init("nccl" if args.impl == "ours" else "gloo")
     return world, rank, local, dist
 
 
@@ -212,7 +207,7 @@ def reference_arm(args, world, rank):
         total += mbs
     value = total / sum(times)
     sample = f"{len(streams)} streams x {frames} pictures to bitstreams per step (oracle, C, -O2)"
-    line = {"impl": "reference", "metric": "encoded MB/s", "value": value, "unit": "MB/s", "n_gpus": args.gpus,
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "MB/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
             "config": {"workload": args.workload, "streams": len(streams), "mb_per_step": total // args.steps},
@@ -302,11 +297,11 @@ class Runner:
 
 def ours(args, world, rank, local, dist):
     import torch
-    from h261enc_cuda_b200 import workloads
+    from h261enc_cuda_b200 import shard
     from h261enc_cuda_b200.engine import Engine, sad_peak
 
     torch.cuda.set_device(local)
-    streams = workloads.WORKLOADS[args.workload](rank=rank)
+    streams = shard.rank_streams(args.workload, rank)
     mb_per_step = sum(s.num_mb for s in streams)
     pools = device_clips(streams, CLIP_LEN, local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
@@ -341,11 +336,7 @@ def ours(args, world, rank, local, dist):
             bits_bytes.append(eng.step_bits()[0])
             run.retire(run.queued - 1)
     torch.cuda.synchronize()
-    total_ms = float(sum(kernel_ms) + sum(bits_ms))
-    if dist:
-        t = torch.tensor([total_ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = shard.max_over_ranks(float(sum(kernel_ms) + sum(bits_ms)), dist, f"cuda:{local}")
     value = mb_per_step * args.steps * world / (total_ms * 1e-3)
 
     # ---- e2e: host pictures in, bitstreams out, through the public API.
@@ -385,11 +376,7 @@ def ours(args, world, rank, local, dist):
     eng.sync()
     consume(args.steps - 1)
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = shard.max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
     e2e = mb_per_step * args.steps * world / e2e_s
     h2d //= args.steps
     d2h //= args.steps
@@ -428,7 +415,7 @@ def ours(args, world, rank, local, dist):
     tr = ncu_traffic_per_mb()
     sad_rate = mb_per_step * SAD_PER_MB / (mean_kernel * 1e-3)
     line = {
-        "metric": "encoded MB/s (batched 64 mixed QCIF/CIF streams to H.261 bitstreams, bit-exact to the reference)",
+        "metric": METRIC,
         "value": value, "unit": "MB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": mean_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u8", "data": "synthetic (seeded pan/object clips, 24-picture ping-pong per stream)",
@@ -470,7 +457,7 @@ def serve(args, world, rank, local, dist):
     under a 40 GB HBM budget; aggregate MB/s and per-picture latency over
     the run."""
     import torch
-    from h261enc_cuda_b200 import serving
+    from h261enc_cuda_b200 import serving, shard
     from h261enc_cuda_b200.engine import Engine
 
     torch.cuda.set_device(local)
@@ -483,11 +470,7 @@ def serve(args, world, rank, local, dist):
         with ClockSampler(local) as clk:
             st = srv.run(reqs, duration=args.serve_seconds)
     summ = st.summary()
-    value = st.macroblocks / st.duration
-    if dist:
-        t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t)
-        value = float(t.item())
+    value = shard.sum_over_ranks(st.macroblocks / st.duration, dist, f"cuda:{local}")
     if rank == 0:
         line = {"metric": "served encoded MB/s (Poisson 200 sessions/s, 30 fps each, HBM-budget admission)",
                 "value": value, "unit": "MB/s", "n_gpus": world, "steps": st.steps, "warmup": 0,
