@@ -1284,6 +1284,8 @@ extern "C" int h261b_engine_step_pictures(h261b_engine_t *e, int32_t cap, h261b_
         const h261b_pic_info_t &pi = *(const h261b_pic_info_t *)(rm.host + r.pic_off);
         if (pi.status == 0 && pi.host_off >= 0)
             span = std::max<int64_t>(span, (int64_t)pi.host_off + ((pi.bytes + 15) & ~15));
+        if (pi.status == 0 && pi.host_off < 0)
+            e->bits_want = std::max(e->bits_want, 2 * e->bits[p].cap);   /* later steps fit */
         if (n < cap) {
             h261b_picture_t &o = out[n];
             o.session_id = (int32_t)i;
