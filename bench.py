@@ -153,15 +153,37 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def ncu_traffic_per_mb():
-    """DRAM bytes per MB of the step kernel from the committed ncu summary."""
+def ncu_figure(key):
+    """A per-MB figure of the step kernel from the committed ncu summary."""
     try:
         for line in open(PROFILE_SUMMARY):
-            if line.startswith("dram_bytes_per_mb:"):
+            if line.startswith(key + ":"):
                 return float(line.split(":")[1])
     except OSError:
         pass
     return None
+
+
+def ncu_traffic_per_mb():
+    """DRAM bytes per MB of the step kernel (ncu)."""
+    return ncu_figure("dram_bytes_per_mb")
+
+
+def issue_roofline(mb_per_step, kernel_ms, device, clocks):
+    """The encode kernel is issue-bound (integer SIMD search, exact float
+    transforms), so its roofline is the SM issue rate: warp instructions per
+    MB (ncu, committed summary) x MBs per step / kernel time, against 4 warp
+    instructions per cycle per SM x SMs x the median SM clock measured."""
+    import torch
+    ipm = ncu_figure("warp_instr_per_mb")
+    mhz = clocks.get("sm_mhz")
+    if ipm is None or not mhz:
+        return None
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    achieved = ipm * mb_per_step / (kernel_ms * 1e-3)
+    peak = 4.0 * sms * mhz * 1e6
+    return {"achieved": achieved, "peak": peak, "unit": "warp instructions/s", "frac": achieved / peak,
+            "instructions_per_mb": ipm, "peak_source": f"4 per cycle x {sms} SMs x {mhz:.0f} MHz (measured)"}
 
 
 def dist_setup(args):
@@ -452,6 +474,9 @@ def ours(args, world, rank, local, dist):
                      "traffic": (tr * mb_per_step) if tr else None},
         "sad_roofline": {"achieved": sad_rate, "peak": peak_sad, "unit": "absdiff/s", "frac": sad_rate / peak_sad,
                          "peak_source": "project microbenchmark of the search's SAD step"},
+        # the committed ncu figure is for batch64
+        "issue_roofline": (issue_roofline(mb_per_step, mean_kernel, local, clk.summary())
+                           if args.workload == "batch64" else None),
         "gpu_launches": 5 * args.steps,   # encode + codes, layout, pack, copy
         "clocks": clk.summary(),
     }

@@ -594,7 +594,9 @@ extern "C" int h261b_launch_bitstream(h261b_session_dev_t *sessions_dev, int32_t
 {
     if (n_work <= 0 || n_sessions <= 0)
         return 0;
-    const int ctas = (int)std::min<int64_t>((n_work + 4 * VLC_WARPS - 1) / (4 * VLC_WARPS), (int64_t)sm_count * 4);
+    /* two MBs per warp, up to eight CTAs per SM: latency-bound kernels want
+     * every warp slot they can get */
+    const int ctas = (int)std::min<int64_t>((n_work + 2 * VLC_WARPS - 1) / (2 * VLC_WARPS), (int64_t)sm_count * 8);
     cudaStream_t st = (cudaStream_t)stream;
     codes_kernel<<<ctas, VLC_THREADS, 0, st>>>(sessions_dev, work_dev, n_work);
     layout_kernel<<<n_sessions, VLC_THREADS, 0, st>>>(sessions_dev);
