@@ -26,8 +26,9 @@
  *   pack    every coded macroblock writes its header and shifts its bit
  *           string into place; a macroblock's first and last word can be
  *           shared with its neighbours and are ORed in with atomics.
- *   copy    one CTA per picture copies it into the host arena (mapped
- *           pinned memory) at an offset drawn with one atomic.
+ *   copy    the picture into the host arena (mapped pinned memory), at
+ *           the offset layout drew with one atomic, split over several
+ *           CTAs per picture.
  */
 #include <cuda_runtime.h>
 #include <stddef.h>
@@ -320,8 +321,14 @@ __global__ void __launch_bounds__(VLC_THREADS) codes_kernel(const h261b_session_
     }
 }
 
-/* ---- layout: one CTA per picture, a warp per GOB */
-__global__ void __launch_bounds__(VLC_THREADS) layout_kernel(const h261b_session_dev_t *sessions)
+/* ---- layout: one CTA per picture, a warp per GOB (12 warps: all of a CIF
+ * picture's GOBs at once); it also draws the picture's place in the host
+ * arena, so that the copy can be split over several CTAs */
+constexpr int LAYOUT_THREADS = 12 * 32;
+constexpr int COPY_SPLIT = 8;
+
+__global__ void __launch_bounds__(LAYOUT_THREADS) layout_kernel(const h261b_session_dev_t *sessions,
+                                                                h261b_step_dev_t *step, int64_t host_cap)
 {
     const h261b_session_dev_t &S = sessions[blockIdx.x];
     if (!S.bits_out)
@@ -339,7 +346,8 @@ __global__ void __launch_bounds__(VLC_THREADS) layout_kernel(const h261b_session
         bad = 0;
     __syncthreads();
 
-    for (int g = warp; g < ngob; g += VLC_WARPS) {
+    const int nwarps = blockDim.x >> 5;
+    for (int g = warp; g < ngob; g += nwarps) {
         const int x0 = cif ? (g & 1) * 11 : 0, y0 = (cif ? g >> 1 : g) * 3;
         const int mi = (y0 + lane / 11) * S.mbw + x0 + lane % 11;
         const int m32 = (y0 + 2) * S.mbw + x0 + 10;
@@ -404,12 +412,12 @@ __global__ void __launch_bounds__(VLC_THREADS) layout_kernel(const h261b_session
     const int64_t words = ((total + 127) / 128) * 4;   /* whole 16-byte units */
     const int status = bad ? H261B_BITS_BAD_RECORD : (words * 4 > S.bits_cap ? H261B_BITS_OVERFLOW : 0);
     if (status == 0) {
-        for (int i = tid; i < nmb; i += VLC_THREADS) {
+        for (int i = tid; i < nmb; i += (int)blockDim.x) {
             const int mbx = i % S.mbw, mby = i / S.mbw;
             const int g = cif ? (mby / 3) * 2 + mbx / 11 : mby / 3;
             S.vlc_pos[i] = (int32_t)(gob_start[g] + rel[i]);
         }
-        for (int64_t i = tid; i < words; i += VLC_THREADS)
+        for (int64_t i = tid; i < words; i += (int)blockDim.x)
             S.bits_out[i] = 0u;
     }
     __syncthreads();
@@ -432,6 +440,15 @@ __global__ void __launch_bounds__(VLC_THREADS) layout_kernel(const h261b_session
     if (tid == 0) {
         S.vlc_total[0] = (int32_t)total;
         S.vlc_total[1] = status != 0 ? status : (any_oob ? H261B_BITS_MISMATCH : 0);
+        /* the picture's place in the host arena */
+        int32_t off = -1;
+        if (S.vlc_total[1] == 0 && host_cap > 0) {
+            const uint32_t padded = (uint32_t)((((total + 7) >> 3) + 15) & ~15);
+            const uint32_t a = atomicAdd(&step->host_used, padded);
+            if ((int64_t)a + padded <= host_cap)
+                off = (int32_t)a;
+        }
+        S.vlc_total[2] = off;
         /* the rate control learns the picture's size */
         if (S.rc && S.vlc_total[1] == 0)
             rc_update(*S.rc, S.frame_type, (int32_t)((total + 7) >> 3));
@@ -530,37 +547,28 @@ __global__ void __launch_bounds__(VLC_THREADS) pack_kernel(const h261b_session_d
     }
 }
 
-/* ---- copy: each picture into the host arena */
-__global__ void __launch_bounds__(VLC_THREADS) copy_kernel(const h261b_session_dev_t *sessions,
-                                                           h261b_step_dev_t *step, uint8_t *host_arena,
-                                                           int64_t host_cap)
+/* ---- copy: each picture into the host arena, COPY_SPLIT CTAs per picture */
+__global__ void __launch_bounds__(VLC_THREADS) copy_kernel(const h261b_session_dev_t *sessions, uint8_t *host_arena)
 {
     const h261b_session_dev_t &S = sessions[blockIdx.x];
     if (!S.bits_out)
         return;
-    __shared__ int off;
     const int total = S.vlc_total[0];
     const int64_t words = ((int64_t)(total + 127) / 128) * 4;
     const int st = (total < 0 || words * 4 > S.bits_cap) ? H261B_BITS_OVERFLOW : S.vlc_total[1];
+    const int off = st == 0 ? S.vlc_total[2] : -1;
     const int bytes = (total + 7) >> 3;
-    const int padded = (bytes + 15) & ~15;
-    if (threadIdx.x == 0) {
-        int o = -1;
-        if (st == 0 && host_arena) {
-            const uint32_t a = atomicAdd(&step->host_used, (uint32_t)padded);
-            if ((int64_t)a + padded <= host_cap)
-                o = (int)a;
-        }
-        off = o;
-        *S.pic_out = h261b_pic_info_t{ st == 0 ? bytes : 0, o, st, S.rc ? S.rc->picture_quant : S.quant };
-    }
-    __syncthreads();
-    if (off >= 0) {
-        const uint4 *s4 = reinterpret_cast<const uint4 *>(S.bits_out);
-        uint4 *d4 = reinterpret_cast<uint4 *>(host_arena + off);
-        for (int i = threadIdx.x; i < padded / 16; i += VLC_THREADS)
-            d4[i] = s4[i];
-    }
+    const int units = ((bytes + 15) & ~15) / 16;
+    if (blockIdx.y == 0 && threadIdx.x == 0)
+        *S.pic_out = h261b_pic_info_t{ st == 0 ? bytes : 0, off, st, S.rc ? S.rc->picture_quant : S.quant };
+    if (off < 0 || !host_arena)
+        return;
+    const int per = (units + COPY_SPLIT - 1) / COPY_SPLIT;
+    const int lo = blockIdx.y * per, hi = min(units, lo + per);
+    const uint4 *s4 = reinterpret_cast<const uint4 *>(S.bits_out);
+    uint4 *d4 = reinterpret_cast<uint4 *>(host_arena + off);
+    for (int i = lo + (int)threadIdx.x; i < hi; i += VLC_THREADS)
+        d4[i] = s4[i];
 }
 
 } // namespace
@@ -599,7 +607,7 @@ extern "C" int h261b_launch_bitstream(h261b_session_dev_t *sessions_dev, int32_t
     const int ctas = (int)std::min<int64_t>((n_work + 2 * VLC_WARPS - 1) / (2 * VLC_WARPS), (int64_t)sm_count * 8);
     cudaStream_t st = (cudaStream_t)stream;
     codes_kernel<<<ctas, VLC_THREADS, 0, st>>>(sessions_dev, work_dev, n_work);
-    layout_kernel<<<n_sessions, VLC_THREADS, 0, st>>>(sessions_dev);
+    layout_kernel<<<n_sessions, LAYOUT_THREADS, 0, st>>>(sessions_dev, step, host_arena_dev ? host_cap : 0);
     if (layout_done_event) {
         /* the next step's rate control reads what the layout updated */
         const cudaError_t err = cudaEventRecord((cudaEvent_t)layout_done_event, st);
@@ -607,6 +615,6 @@ extern "C" int h261b_launch_bitstream(h261b_session_dev_t *sessions_dev, int32_t
             return (int)err;
     }
     pack_kernel<<<ctas, VLC_THREADS, 0, st>>>(sessions_dev, work_dev, n_work);
-    copy_kernel<<<n_sessions, VLC_THREADS, 0, st>>>(sessions_dev, step, host_arena_dev, host_cap);
+    copy_kernel<<<dim3(n_sessions, COPY_SPLIT), VLC_THREADS, 0, st>>>(sessions_dev, host_arena_dev);
     return (int)cudaGetLastError();
 }
