@@ -415,6 +415,7 @@ def ours(args, world, rank, local, dist):
     e2e = mb_per_step * args.steps * world / e2e_s
     h2d //= args.steps
     d2h //= args.steps
+    graph_caps, graph_reps = eng.graph_stats()
     eng.destroy()
 
     # ---- single stream: the same streams one at a time, one picture per step
@@ -478,6 +479,8 @@ def ours(args, world, rank, local, dist):
         "issue_roofline": (issue_roofline(mb_per_step, mean_kernel, local, clk.summary())
                            if args.workload == "batch64" else None),
         "gpu_launches": 5 * args.steps,   # encode + codes, layout, pack, copy
+        "graphs": {"captures": graph_caps, "replays": graph_reps,
+                   "note": "steps whose launch signature repeats replay a captured CUDA graph"},
         "clocks": clk.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:

@@ -65,7 +65,7 @@ class EngineConfig(Structure):
     _fields_ = [("device", c_int32), ("max_sessions", c_int32), ("hbm_budget_bytes", c_int64),
                 ("me_mode", c_int32), ("fmad", c_int32), ("warps_per_cta", c_int32),
                 ("max_ctas", c_int32), ("copy_threads", c_int32), ("levels_to_host", c_int32),
-                ("bits_host_bytes", c_int64)]
+                ("bits_host_bytes", c_int64), ("use_graphs", c_int32), ("reserved", c_int32)]
 
 
 class SessionConfig(Structure):
@@ -128,6 +128,8 @@ def core() -> ctypes.CDLL:
         lib.h261b_engine_submit_batch.argtypes = [c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
                                                   c_void_p]
         lib.h261b_engine_submit_batch_async.argtypes = lib.h261b_engine_submit_batch.argtypes
+        lib.h261b_engine_graph_stats.argtypes = [c_void_p, POINTER(c_int64), POINTER(c_int64)]
+        lib.h261b_engine_launch_shape.argtypes = [c_void_p, POINTER(c_int32), POINTER(c_int32), POINTER(c_int32)]
         lib.h261b_engine_step_timing.argtypes = [c_void_p, POINTER(StepTiming)]
         lib.h261b_engine_last_bits_ms.argtypes = [c_void_p, POINTER(c_float)]
         lib.h261b_engine_step_pictures.argtypes = [c_void_p, c_int32, c_void_p, POINTER(c_int32),

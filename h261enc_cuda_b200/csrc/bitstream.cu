@@ -610,7 +610,12 @@ extern "C" int h261b_launch_bitstream(h261b_session_dev_t *sessions_dev, int32_t
     layout_kernel<<<n_sessions, LAYOUT_THREADS, 0, st>>>(sessions_dev, step, host_arena_dev ? host_cap : 0);
     if (layout_done_event) {
         /* the next step's rate control reads what the layout updated */
-        const cudaError_t err = cudaEventRecord((cudaEvent_t)layout_done_event, st);
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaError_t err = cudaStreamIsCapturing(st, &cs);
+        if (err == cudaSuccess)
+            err = cudaEventRecordWithFlags((cudaEvent_t)layout_done_event, st,
+                                           cs == cudaStreamCaptureStatusActive ? cudaEventRecordExternal
+                                                                               : cudaEventRecordDefault);
         if (err != cudaSuccess)
             return (int)err;
     }

@@ -28,6 +28,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -129,6 +130,26 @@ struct Mirror {
             cudaFree(dev);
         host = dev = nullptr;
         cap = 0;
+    }
+};
+
+/* everything about a step's launches that a captured graph bakes in */
+struct StepKey {
+    const void *dm_host, *dm_dev, *um_host, *um_dev, *rm_host, *rm_dev, *bits_dev;
+    size_t bits_cap, desc_off, work_off, desc_bytes, upload_bytes, ssd_base, d2h;
+    int64_t n;
+    int32_t n_work, rc_begin, n_rc, ssd, warps, ctas, phases, waits;
+    bool operator==(const StepKey &o) const { return memcmp(this, &o, sizeof(StepKey)) == 0; }
+};
+
+struct StepGraph {
+    cudaGraphExec_t exec = nullptr;
+    StepKey key;
+    void reset()
+    {
+        if (exec)
+            cudaGraphExecDestroy(exec);
+        exec = nullptr;
     }
 };
 
@@ -257,13 +278,24 @@ struct h261b_engine_s {
     std::unique_ptr<CopyPool> copier;   /* batched submissions */
     std::vector<CopyJob> copy_jobs;
 
+    /* graph replay of steps (use_graphs) */
+    StepGraph graph[2];
+    bool graphs_off = false;
+    int64_t graph_captures = 0, graph_replays = 0;
+
     /* launch tuning */
     int warps = 4, ctas = 0;
     std::vector<std::pair<int, int>> tune_cands;
     std::vector<float> tune_ms;
     size_t tune_next = 0;
     bool tuned = false;
+    int shape_source = 0;   /* 0 configured, 1 tuned here, 2 tuned earlier in this process */
 };
+
+/* the launch shape tuning chose, per device, for the engines created after
+ * it in this process */
+static std::mutex g_tuned_mu;
+static std::map<int, std::pair<int, int>> g_tuned;
 
 static const char *k_version = "h261b 0.2 (sm_100a)";
 
@@ -283,6 +315,7 @@ extern "C" void h261b_engine_config_default(h261b_engine_config_t *c)
     c->copy_threads = 0;
     c->levels_to_host = 1;
     c->bits_host_bytes = 0;
+    c->use_graphs = 1;
 }
 
 extern "C" int64_t h261b_session_bytes(int32_t w, int32_t h)
@@ -387,11 +420,23 @@ extern "C" int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engin
         return H261B_ERR_CUDA;
     }
     e->sm_count = prop.multiProcessorCount;
+    bool cached = false;
+    if (cfg->warps_per_cta == 0) {
+        std::lock_guard<std::mutex> lk(g_tuned_mu);
+        auto it = g_tuned.find(cfg->device);
+        if (it != g_tuned.end()) {
+            e->warps = it->second.first;
+            e->ctas = it->second.second;
+            e->tuned = true;
+            e->shape_source = 2;
+            cached = true;
+        }
+    }
     if (cfg->warps_per_cta > 0) {
         e->warps = cfg->warps_per_cta;
         e->ctas = cfg->max_ctas;
         e->tuned = true;
-    } else {
+    } else if (!cached) {
         /* launch shapes tried on the first steps: warps per CTA, each with a
          * grid of one wave of resident CTAs */
         const int wl[4] = { 2, 4, 8, 4 };
@@ -413,6 +458,7 @@ extern "C" int h261b_engine_destroy(h261b_engine_t *e)
         if (e->stream[p])
             cudaStreamSynchronize(e->stream[p]);
     for (int p = 0; p < 2; p++) {
+        e->graph[p].reset();
         e->upload[p].release();
         e->results[p].release();
         e->desc[p].release();
@@ -812,6 +858,11 @@ static int next_launch_shape(h261b_engine_t *e, int *warps, int *ctas)
     return 0;
 }
 
+static const void *bits_dev_or_null(h261b_engine_t *e, int p, int32_t n_bits)
+{
+    return n_bits ? (const void *)e->bits[p].dev : nullptr;
+}
+
 extern "C" int h261b_engine_step(h261b_engine_t *e)
 {
     clear_error();
@@ -945,65 +996,116 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
     cudaStream_t st = e->stream[p];
     const size_t desc_bytes = work_off + (size_t)n_work * sizeof(uint32_t);
     e->copier->join();   /* pictures of h261b_engine_submit_batch_async */
-    H261B_CUDA_TRY(cudaEventRecord(e->t_begin[p], st));
-    if (n_ssd)
-        H261B_CUDA_TRY(cudaMemsetAsync(rm.dev + ssd_base, 0, n * 32, st));
-    H261B_CUDA_TRY(cudaMemcpyAsync(dm.dev, dm.host, desc_bytes, cudaMemcpyHostToDevice, st));
-    if (e->upload_checked && e->upload_used)
-        H261B_CUDA_TRY(cudaMemcpyAsync(um.dev, um.host, e->upload_used, cudaMemcpyHostToDevice, st));
-    H261B_CUDA_TRY(cudaEventRecord(e->h2d_done[p], st));
-    H261B_CUDA_TRY(cudaEventRecord(e->t_h2d[p], st));
-    /* the previous step's reconstructions are this step's references */
-    if (id > 0)
-        H261B_CUDA_TRY(cudaStreamWaitEvent(st, e->kernel_done[p ^ 1], 0));
-    H261B_CUDA_TRY(cudaEventRecord(e->t_ready[p], st));
-
     int warps, ctas;
     const int tuning = next_launch_shape(e, &warps, &ctas);
-    H261B_CUDA_TRY(cudaEventRecord(e->k_start[p], st));
     const int phases = H261B_PHASE_ME | H261B_PHASE_MD | H261B_PHASE_ENCDEC | (e->cfg.fmad ? 0x100 : 0);
-    const h261b_session_dev_t *desc_dev = (const h261b_session_dev_t *)(dm.dev + desc_off);
+    h261b_session_dev_t *desc_dev = (h261b_session_dev_t *)(dm.dev + desc_off);
     const uint32_t *work_dev = (const uint32_t *)(dm.dev + work_off);
-    int lr = h261b_launch_step(desc_dev, work_dev, n_work, phases, warps, ctas, st);
-    if (lr == 0 && n_rc) {
-        /* rate-controlled sessions: the picture QUANT from this picture's
-         * costs and the previous picture's size (written by the previous
-         * step's layout kernel), then their encode */
-        if (id > 0)
-            H261B_CUDA_TRY(cudaStreamWaitEvent(st, e->layout_done[p ^ 1], 0));
-        lr = h261b_launch_ratectrl((h261b_session_dev_t *)(dm.dev + desc_off), (int32_t)n, st);
-        if (lr == 0)
-            lr = h261b_launch_step(desc_dev, work_dev + rc_begin, n_work - rc_begin,
-                                   H261B_PHASE_ENCDEC | (e->cfg.fmad ? 0x100 : 0), warps, ctas, st);
-    }
-    if (lr != 0) {
-        set_error("step launch failed: %s", cudaGetErrorString((cudaError_t)lr));
-        return H261B_ERR_CUDA;
-    }
-    H261B_CUDA_TRY(cudaEventRecord(e->k_end[p], st));
-    /* the next step may start encoding while this one writes bitstreams */
-    H261B_CUDA_TRY(cudaEventRecord(e->kernel_done[p], st));
-    if (n_bits) {
-        if ((rc = e->bits[p].reserve(e->bits_want)))
-            return rc;
-        lr = h261b_launch_bitstream((h261b_session_dev_t *)(dm.dev + desc_off), (int32_t)n,
-                                    (const uint32_t *)(dm.dev + work_off), n_work, (h261b_step_dev_t *)dm.dev,
-                                    e->bits[p].dev, (int64_t)e->bits[p].cap, e->sm_count, st,
-                                    (void *)e->layout_done[p]);
-        if (lr != 0) {
-            set_error("bitstream launch failed: %s", cudaGetErrorString((cudaError_t)lr));
-            return H261B_ERR_CUDA;
-        }
-        H261B_CUDA_TRY(cudaEventRecord(e->b_end[p], st));
-    }
-    e->step_bits_ran[p] = n_bits > 0;
+    const size_t upload_bytes = e->upload_checked ? e->upload_used : 0;
     /* records and picture records always, levels when asked for */
     const size_t d2h = e->cfg.levels_to_host ? res_off : levels_base;
-    H261B_CUDA_TRY(cudaMemcpyAsync(rm.host, rm.dev, d2h, cudaMemcpyDeviceToHost, st));
-    e->last_h2d = (int64_t)desc_bytes + (e->upload_checked ? (int64_t)e->upload_used : 0);
+    if (n_bits && (rc = e->bits[p].reserve(e->bits_want)))
+        return rc;
+
+    /* the step's device work: uploads, encode (and rate control), the
+     * bitstream kernels, the download, and the events the host and the
+     * other stream wait on.  Recorded as external events so that a graph
+     * captured from it keeps them visible outside the graph. */
+    auto enqueue = [&](bool capturing) -> int {
+        const unsigned rf = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+        const unsigned wf = capturing ? cudaEventWaitExternal : cudaEventWaitDefault;
+        H261B_CUDA_TRY(cudaEventRecordWithFlags(e->t_begin[p], st, rf));
+        if (n_ssd)
+            H261B_CUDA_TRY(cudaMemsetAsync(rm.dev + ssd_base, 0, n * 32, st));
+        H261B_CUDA_TRY(cudaMemcpyAsync(dm.dev, dm.host, desc_bytes, cudaMemcpyHostToDevice, st));
+        if (upload_bytes)
+            H261B_CUDA_TRY(cudaMemcpyAsync(um.dev, um.host, upload_bytes, cudaMemcpyHostToDevice, st));
+        H261B_CUDA_TRY(cudaEventRecordWithFlags(e->h2d_done[p], st, rf));
+        H261B_CUDA_TRY(cudaEventRecordWithFlags(e->t_h2d[p], st, rf));
+        /* the previous step's reconstructions are this step's references */
+        if (id > 0)
+            H261B_CUDA_TRY(cudaStreamWaitEvent(st, e->kernel_done[p ^ 1], wf));
+        H261B_CUDA_TRY(cudaEventRecordWithFlags(e->t_ready[p], st, rf));
+        H261B_CUDA_TRY(cudaEventRecordWithFlags(e->k_start[p], st, rf));
+        int lr = h261b_launch_step(desc_dev, work_dev, n_work, phases, warps, ctas, st);
+        if (lr == 0 && n_rc) {
+            /* rate-controlled sessions: the picture QUANT from this
+             * picture's costs and the previous picture's size (written by
+             * the previous step's layout kernel), then their encode */
+            if (id > 0)
+                H261B_CUDA_TRY(cudaStreamWaitEvent(st, e->layout_done[p ^ 1], wf));
+            lr = h261b_launch_ratectrl(desc_dev, (int32_t)n, st);
+            if (lr == 0)
+                lr = h261b_launch_step(desc_dev, work_dev + rc_begin, n_work - rc_begin,
+                                       H261B_PHASE_ENCDEC | (e->cfg.fmad ? 0x100 : 0), warps, ctas, st);
+        }
+        if (lr != 0) {
+            set_error("step launch failed: %s", cudaGetErrorString((cudaError_t)lr));
+            return H261B_ERR_CUDA;
+        }
+        H261B_CUDA_TRY(cudaEventRecordWithFlags(e->k_end[p], st, rf));
+        /* the next step may start encoding while this one writes bitstreams */
+        H261B_CUDA_TRY(cudaEventRecordWithFlags(e->kernel_done[p], st, rf));
+        if (n_bits) {
+            lr = h261b_launch_bitstream(desc_dev, (int32_t)n, work_dev, n_work, (h261b_step_dev_t *)dm.dev,
+                                        e->bits[p].dev, (int64_t)e->bits[p].cap, e->sm_count, st,
+                                        (void *)e->layout_done[p]);
+            if (lr != 0) {
+                set_error("bitstream launch failed: %s", cudaGetErrorString((cudaError_t)lr));
+                return H261B_ERR_CUDA;
+            }
+            H261B_CUDA_TRY(cudaEventRecordWithFlags(e->b_end[p], st, rf));
+        }
+        H261B_CUDA_TRY(cudaMemcpyAsync(rm.host, rm.dev, d2h, cudaMemcpyDeviceToHost, st));
+        H261B_CUDA_TRY(cudaEventRecordWithFlags(e->t_end[p], st, rf));
+        H261B_CUDA_TRY(cudaEventRecordWithFlags(e->step_done[p], st, rf));
+        return H261B_OK;
+    };
+
+    /* Steps whose launches look the same (sizes, arena addresses, launch
+     * shape) replay one CUDA graph per parity: the descriptor and work-list
+     * contents differ, but they are data in pinned memory that the graph's
+     * upload copies.  Tuning steps, an engine's first step and engines with
+     * use_graphs = 0 launch directly. */
+    const StepKey key = { dm.host, dm.dev, um.host, um.dev, rm.host, rm.dev, bits_dev_or_null(e, p, n_bits),
+                          n_bits ? e->bits[p].cap : 0, desc_off, work_off, desc_bytes, upload_bytes, ssd_base,
+                          d2h, (int64_t)n, n_work, rc_begin, n_rc, n_ssd ? 1 : 0, warps, ctas, phases,
+                          id > 0 ? 1 : 0 };
+    StepGraph &gr = e->graph[p];
+    const bool capturable = e->cfg.use_graphs && !e->graphs_off && !tuning && id > 0;
+    if (capturable && gr.exec && gr.key == key) {
+        H261B_CUDA_TRY(cudaGraphLaunch(gr.exec, st));
+        e->graph_replays++;
+    } else if (capturable && cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        const int erc = enqueue(true);
+        cudaGraph_t g = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(st, &g);
+        cudaGraphExec_t ex = nullptr;
+        if (erc == H261B_OK && ce == cudaSuccess && g)
+            ce = cudaGraphInstantiate(&ex, g, 0);
+        if (g)
+            cudaGraphDestroy(g);
+        if (erc != H261B_OK || ce != cudaSuccess || !ex) {
+            /* capture did not work here: nothing of it ran; launch directly
+             * from now on */
+            cudaGetLastError();
+            e->graphs_off = true;
+            if ((rc = enqueue(false)))
+                return rc;
+        } else {
+            gr.reset();
+            gr.exec = ex;
+            gr.key = key;
+            H261B_CUDA_TRY(cudaGraphLaunch(ex, st));
+            e->graph_captures++;
+        }
+    } else {
+        if ((rc = enqueue(false)))
+            return rc;
+    }
+    e->step_bits_ran[p] = n_bits > 0;
+    e->last_h2d = (int64_t)desc_bytes + (int64_t)upload_bytes;
     e->last_d2h = (int64_t)d2h;
-    H261B_CUDA_TRY(cudaEventRecord(e->t_end[p], st));
-    H261B_CUDA_TRY(cudaEventRecord(e->step_done[p], st));
     e->in_flight[p] = true;
     e->step_mbs[p] = total_mb;
 
@@ -1022,6 +1124,9 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
             e->warps = e->tune_cands[best].first;
             e->ctas = e->tune_cands[best].second;
             e->tuned = true;
+            e->shape_source = 1;
+            std::lock_guard<std::mutex> lk(g_tuned_mu);
+            g_tuned[e->cfg.device] = { e->warps, e->ctas };
         }
     }
 
@@ -1301,6 +1406,26 @@ extern "C" int h261b_engine_step_pictures(h261b_engine_t *e, int32_t cap, h261b_
         *arena = e->bits[p].host;
     if (arena_bytes)
         *arena_bytes = span;
+    return H261B_OK;
+}
+
+extern "C" int h261b_engine_graph_stats(h261b_engine_t *e, int64_t *captures, int64_t *replays)
+{
+    if (!e || !captures || !replays)
+        return H261B_ERR_ARG;
+    *captures = e->graph_captures;
+    *replays = e->graph_replays;
+    return H261B_OK;
+}
+
+extern "C" int h261b_engine_launch_shape(h261b_engine_t *e, int32_t *warps_per_cta, int32_t *max_ctas,
+                                         int32_t *source)
+{
+    if (!e || !warps_per_cta || !max_ctas || !source)
+        return H261B_ERR_ARG;
+    *warps_per_cta = e->warps;
+    *max_ctas = e->ctas;
+    *source = e->shape_source;
     return H261B_OK;
 }
 

@@ -52,7 +52,8 @@ class FrameResult:
 class Engine:
     def __init__(self, device: int = 0, max_sessions: int = 4096, hbm_budget_bytes: int = 0,
                  me_mode: int = 0, fmad: int = 1, warps_per_cta: int = 0, max_ctas: int = 0,
-                 copy_threads: int = 0, levels_to_host: int = 1, bits_host_bytes: int = 0):
+                 copy_threads: int = 0, levels_to_host: int = 1, bits_host_bytes: int = 0,
+                 use_graphs: int = 1):
         lib = _lib.core()
         cfg = _lib.EngineConfig()
         lib.h261b_engine_config_default(ctypes.byref(cfg))
@@ -60,6 +61,7 @@ class Engine:
         cfg.me_mode, cfg.fmad, cfg.warps_per_cta, cfg.max_ctas = me_mode, fmad, warps_per_cta, max_ctas
         cfg.copy_threads = copy_threads
         cfg.levels_to_host, cfg.bits_host_bytes = levels_to_host, bits_host_bytes
+        cfg.use_graphs = use_graphs
         h = ctypes.c_void_p()
         check(lib.h261b_engine_create(ctypes.byref(cfg), ctypes.byref(h)), "h261b_engine_create")
         self._h = h
@@ -199,6 +201,21 @@ class Engine:
         span = (np.ctypeslib.as_array((ctypes.c_uint8 * used.value).from_address(base.value))
                 if used.value else np.empty(0, np.uint8))
         return out[:min(n.value, cap)], span
+
+    def graph_stats(self):
+        """(steps captured as CUDA graphs, steps that replayed one)."""
+        a, b = ctypes.c_int64(), ctypes.c_int64()
+        check(_lib.core().h261b_engine_graph_stats(self._h, ctypes.byref(a), ctypes.byref(b)),
+              "h261b_engine_graph_stats")
+        return a.value, b.value
+
+    def launch_shape(self):
+        """(warps per CTA, CTA cap, source: 0 configured, 1 tuned, 2 tuned
+        earlier in this process on the same device)."""
+        w, c, src = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        check(_lib.core().h261b_engine_launch_shape(self._h, ctypes.byref(w), ctypes.byref(c), ctypes.byref(src)),
+              "h261b_engine_launch_shape")
+        return w.value, c.value, src.value
 
     def step_timing(self) -> dict:
         """Device timeline of the latest completed step, in milliseconds."""

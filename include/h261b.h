@@ -68,6 +68,10 @@ typedef struct {
     int64_t bits_host_bytes;  /* initial size of each of the two host
                                  bitstream arenas, 0 = 8 MiB; grows when a
                                  step's pictures do not fit                 */
+    int32_t use_graphs;       /* 1 (default): a step whose launches look like
+                                 an earlier one's (sizes, arenas, launch
+                                 shape) replays that step's CUDA graph      */
+    int32_t reserved;
 } h261b_engine_config_t;
 
 void h261b_engine_config_default(h261b_engine_config_t *cfg);
@@ -242,6 +246,14 @@ typedef struct {
     float reserved;
 } h261b_step_timing_t;
 int h261b_engine_step_timing(h261b_engine_t *e, h261b_step_timing_t *t);
+
+/* Steps captured as CUDA graphs and steps that replayed one. */
+int h261b_engine_graph_stats(h261b_engine_t *e, int64_t *captures, int64_t *replays);
+/* The launch shape of the encode kernel (warps per CTA, CTA cap; 0 = one
+ * wave) and whether it came from tuning (1), from a tuning of an earlier
+ * engine on the same device in this process (2) or from the configuration
+ * (0). */
+int h261b_engine_launch_shape(h261b_engine_t *e, int32_t *warps_per_cta, int32_t *max_ctas, int32_t *source);
 
 /* Device time of the last step's encode kernel, and of its bitstream
  * kernel (0 without bitstream sessions), in milliseconds (CUDA events). */

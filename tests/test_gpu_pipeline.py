@@ -141,3 +141,45 @@ def test_step_records_before_any_step(gpu):
     with Engine(warps_per_cta=4) as e:
         step, recs = e.step_records()
         assert step == -1 and recs.size == 0 and recs.dtype == _lib.RESULT_DTYPE
+
+
+@pytest.mark.parametrize("preset", [2, 1])
+def test_graph_replay_equals_direct_launches(gpu, preset):
+    """Steps replayed from captured CUDA graphs produce what directly
+    launched steps produce: records, bitstreams and reconstructions, with
+    sessions of two sizes, one of them rate-controlled."""
+    specs = [(176, 144, 8, 0), (352, 288, 12, 0), (352, 288, 10, 256000)]
+    clips = [synth.clip(preset, w, h, 70 + k, 7) for k, (w, h, q, b) in enumerate(specs)]
+    out = {}
+    for graphs in (0, 1):
+        got = []
+        with Engine(warps_per_cta=4, use_graphs=graphs) as e:
+            sids = [e.open(w, h, q, bitstream=1, rate_control=1 if b else 0, bitrate=b) for (w, h, q, b) in specs]
+            for i in range(clips[0].shape[0]):
+                e.submit_frames(sids, [c[i] for c in clips])
+                e.step()
+                e.sync()
+                for sid in sids:
+                    r = e.result(sid)
+                    got.append((r.mbs.tobytes(), r.bits, np.concatenate(e.recon(sid)).tobytes()))
+            caps, reps = e.graph_stats()
+        if graphs:
+            assert caps >= 1 and reps >= 3
+        else:
+            assert (caps, reps) == (0, 0)
+        out[graphs] = got
+    assert out[0] == out[1]
+
+
+def test_tuned_launch_shape_is_reused_by_later_engines(gpu):
+    fr = synth.clip(0, 176, 144, 5, 6)
+    with Engine() as e:
+        sid = e.open(176, 144, 8)
+        for i in range(6):
+            e.submit_frame(sid, fr[i])
+            e.step()
+            e.sync()
+        w, c, src = e.launch_shape()
+        assert src in (1, 2) and 1 <= w <= 8
+    with Engine() as e2:
+        assert e2.launch_shape() == (w, c, 2)
