@@ -7,9 +7,10 @@
  * MBs of mostly one session) and, for each MB, runs the phases the launch
  * asks for while the next MB's inputs are already on their way:
  *
- *   stage   cp.async copies of the 46x48 luma search window (rows mb_y-15 ..
- *           +30, columns mb_x-16 .. +31) and of the source MB into one of
- *           two per-warp shared-memory buffers, issued one MB ahead.
+ *   stage   16-byte cp.async copies of the 46x48 luma search window (rows
+ *           mb_y-15 .. +30, columns mb_x-16 .. +31) and of the source MB
+ *           into one of two per-warp shared-memory buffers, issued one MB
+ *           ahead.
  *   ME      - reference mode: SAD over the 11x11 coarse grid of
  *             megpu_kernels.cuh:27-166, then the 7x7 refinement of :307-446
  *             around its winner; full mode: every vector of [-15,15]^2;
@@ -46,26 +47,40 @@
 
 namespace {
 
-constexpr int WIN_ROWS = 46;        /* rows mb_y-15 .. mb_y+30               */
-constexpr int WIN_WORDS = 12;       /* columns mb_x-16 .. mb_x+31            */
-constexpr int WIN_PITCH_W = 13;     /* odd word pitch against bank conflicts */
+constexpr int WIN_ROWS = 46;        /* rows mb_y-15 .. mb_y+30; columns mb_x-16 .. mb_x+31 */
+/* A warp's two buffers (this MB, next MB) share 46 rows of 36 words.
+ * Buffer k starts at word 16k of the array and holds, relative to that:
+ *   words 0-11 of row r      window row r (12 words, 48 pixels)
+ *   words 12-15 of row i     source luma row i (i < 16)
+ *   words 12-13 of row 16+j  source chroma row j (Cb j < 8, Cr j >= 8)
+ * so one base pointer addresses all of an MB's inputs.  Rows are 144 B, so
+ * every row and source row is 16-byte aligned for the 16-byte copies, and
+ * with a 36-word pitch the search's lanes, which read rows up to three
+ * apart at up to 13 word columns, meet no bank twice. */
+constexpr int WIN_PITCH_W = 36;
+constexpr int SRC_COL_W = 12;
 constexpr uint32_t FULL = 0xffffffffu;
 
-/* one MB's staged inputs */
-struct __align__(16) StageBuf {
-    uint32_t win[WIN_ROWS * WIN_PITCH_W]; /* reference luma window           */
-    uint32_t pad0[2];
-    uint32_t cur[64];                     /* source luma MB, 16 B per row    */
-    uint32_t curc[2][16];                 /* source Cb, Cr 8x8               */
-};
-
 struct __align__(16) WarpSmem {
-    StageBuf buf[2];                      /* this MB, next MB                */
+    uint32_t buf[WIN_ROWS * WIN_PITCH_W]; /* both buffers, interleaved      */
     float t[4][72];                       /* transpose buffer: row stride 9,
                                              block stride 72 words, so both
                                              row and column accesses of the
                                              four blocks are conflict-free   */
 };
+
+/* one MB's staged inputs: buffer k of the warp's shared memory */
+struct StageBuf {
+    const uint32_t *p;
+    /* window row r from word c */
+    __device__ __forceinline__ const uint32_t *win(int r, int c) const { return p + r * WIN_PITCH_W + c; }
+    /* source luma row i from word c */
+    __device__ __forceinline__ const uint32_t *cur(int i, int c) const { return p + i * WIN_PITCH_W + SRC_COL_W + c; }
+    /* source chroma row j (Cb rows 0-7, Cr rows 8-15), two words */
+    __device__ __forceinline__ const uint32_t *curc(int j) const { return p + (16 + j) * WIN_PITCH_W + SRC_COL_W; }
+};
+
+__device__ __forceinline__ StageBuf stage_view(const WarpSmem &w, int k) { return StageBuf{ w.buf + 16 * k }; }
 
 __constant__ int8_t c_stage1[11] = { -14, -11, -8, -5, -2, 0, 2, 5, 8, 11, 14 };
 /* float tables initialised from double literals like the reference's */
@@ -96,11 +111,12 @@ __device__ __forceinline__ uint32_t compact8(uint32_t v)
 __device__ __forceinline__ uint32_t zorder(uint32_t x, uint32_t y) { return spread8(x) | (spread8(y) << 1); }
 
 /* eight window bytes of row `row` from byte column `col` (any alignment):
- * three word loads, two funnel shifts; col <= 43 keeps the loads inside
- * the row's 13 words (bytes past column 47 are never used) */
-__device__ __forceinline__ uint2 win8(const StageBuf &s, int row, int col)
+ * three word loads, two funnel shifts; 0 <= col <= 43 keeps the loads
+ * inside the row (bytes past column 47, which are the source words or the
+ * other buffer, are never used) */
+__device__ __forceinline__ uint2 win8(const StageBuf s, int row, int col)
 {
-    const uint32_t *p = s.win + row * WIN_PITCH_W + (col >> 2);
+    const uint32_t *p = s.win(row, col >> 2);
     const uint32_t sh = (uint32_t)(col & 3) * 8u;
     const uint32_t a = p[0], b = p[1], c = p[2];
     return make_uint2(__funnelshift_r(a, b, sh), __funnelshift_r(b, c, sh));
@@ -121,14 +137,10 @@ __device__ __forceinline__ int byte8(uint2 v, int i)
     return (int)(((i < 4 ? v.x : v.y) >> (8 * (i & 3))) & 0xFFu);
 }
 
-/* asynchronous global -> shared copies; a source outside the picture is
- * not read (src-size 0) and its bytes are zero-filled */
-__device__ __forceinline__ void cp_async4(void *dst, const void *src, bool valid)
-{
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 4 : 0)
-                 : "memory");
-}
+/* asynchronous global -> shared copies; a 16-byte window chunk outside the
+ * picture is not read (src-size 0) and its bytes are zero-filled.  Window
+ * chunks are cached in L1 too: neighbouring MBs of a warp share two thirds
+ * of them. */
 __device__ __forceinline__ void cp_async8(void *dst, const void *src)
 {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
@@ -138,6 +150,12 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src)
 {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16z(void *dst, const void *src, bool valid)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 16 : 0)
+                 : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
@@ -156,17 +174,17 @@ __device__ __forceinline__ uint32_t sad4(uint32_t a, uint32_t b, uint32_t acc)
 
 /* SADs of the source MB against the window blocks at two vectors, computed
  * together: four accumulators keep the dependency chains short */
-__device__ __forceinline__ void sad16x16_pair(const StageBuf &s, int vx0, int vy0, int vx1, int vy1, uint32_t &s0,
+__device__ __forceinline__ void sad16x16_pair(const StageBuf s, int vx0, int vy0, int vx1, int vy1, uint32_t &s0,
                                               uint32_t &s1)
 {
     const int b0 = 16 + vx0, b1 = 16 + vx1;
-    const uint32_t *p0 = s.win + (15 + vy0) * WIN_PITCH_W + (b0 >> 2);
-    const uint32_t *p1 = s.win + (15 + vy1) * WIN_PITCH_W + (b1 >> 2);
+    const uint32_t *p0 = s.win(15 + vy0, b0 >> 2);
+    const uint32_t *p1 = s.win(15 + vy1, b1 >> 2);
     const uint32_t sh0 = (uint32_t)(b0 & 3) * 8u, sh1 = (uint32_t)(b1 & 3) * 8u;
     uint32_t a0 = 0, a1 = 0, c0 = 0, c1 = 0;
 #pragma unroll 4
     for (int r = 0; r < 16; r++) {
-        const uint4 c = *reinterpret_cast<const uint4 *>(s.cur + 4 * r);
+        const uint4 c = *reinterpret_cast<const uint4 *>(s.cur(r, 0));
         const uint32_t x0 = p0[0], x1 = p0[1], x2 = p0[2], x3 = p0[3], x4 = p0[4];
         const uint32_t y0 = p1[0], y1 = p1[1], y2 = p1[2], y3 = p1[3], y4 = p1[4];
         a0 = sad4(c.x, __funnelshift_r(x0, x1, sh0), a0);
@@ -312,28 +330,39 @@ struct MbDecision {
     int32_t type, flags, mvx, mvy, cost;
 };
 
-/* start the asynchronous copies of one MB's inputs into b */
-__device__ __forceinline__ void stage_mb(StageBuf &b, const h261b_session_dev_t &S, int mbx, int mby, int lane)
+/* start the asynchronous copies of one MB's inputs into buffer k.  The
+ * window is 46 rows of three 16-byte chunks; picture widths are multiples
+ * of 16 and luma planes 16-byte aligned, so a chunk lies wholly inside or
+ * wholly outside the picture, and one outside is zero-filled.  Lanes 0-29
+ * take (row, chunk) = (lane / 3 + 10 i, lane % 3). */
+__device__ __forceinline__ void stage_mb(WarpSmem &w, int k, const h261b_session_dev_t &S, int mbx, int mby,
+                                         int lane)
 {
-    const int W = S.mbw * 16, H = S.mbh * 16;
+    const int H = S.mbh * 16;
     const int x0 = mbx * 16, y0 = mby * 16;
-    for (int t = lane; t < WIN_ROWS * WIN_WORDS; t += 32) {
-        const int r = t / WIN_WORDS, w = t - r * WIN_WORDS;
-        const int y = y0 - 15 + r, x = x0 - 16 + 4 * w;
-        const bool ok = y >= 0 && y < H && x >= 0 && x < W;
-        cp_async4(&b.win[r * WIN_PITCH_W + w], ok ? S.ref_y + (size_t)y * S.pitch_y + x : S.ref_y, ok);
+    uint32_t *base = w.buf + 16 * k;
+    if (lane < 30) {
+        const int j = lane % 3, r0 = lane / 3;
+        const bool xok = j == 1 || (j == 0 ? mbx > 0 : mbx < S.mbw - 1);
+        const int x = x0 - 16 + 16 * j;
+        uint32_t *dst = base + 4 * j;
+        for (int r = r0; r < WIN_ROWS; r += 10) {
+            const int y = y0 - 15 + r;
+            const bool ok = xok && y >= 0 && y < H;
+            cp_async16z(dst + r * WIN_PITCH_W, ok ? S.ref_y + (size_t)y * S.pitch_y + x : S.ref_y, ok);
+        }
     }
     if (lane < 16) {
-        cp_async16(&b.cur[4 * lane], S.cur_y + (size_t)(y0 + lane) * S.pitch_y + x0);
+        cp_async16(base + lane * WIN_PITCH_W + SRC_COL_W, S.cur_y + (size_t)(y0 + lane) * S.pitch_y + x0);
     } else {
-        const int k = lane - 16, pl = k >> 3, r = k & 7;
+        const int q = lane - 16, pl = q >> 3, r = q & 7;
         const uint8_t *src = pl ? S.cur_cr : S.cur_cb;
-        cp_async8(&b.curc[pl][2 * r], src + (size_t)(mby * 8 + r) * S.pitch_c + mbx * 8);
+        cp_async8(base + (16 + q) * WIN_PITCH_W + SRC_COL_W, src + (size_t)(mby * 8 + r) * S.pitch_c + mbx * 8);
     }
 }
 
 /* motion search + SATD costs; results are warp-uniform */
-__device__ __forceinline__ void motion_estimate(const StageBuf &s, const h261b_session_dev_t &S, int mbx, int mby,
+__device__ __forceinline__ void motion_estimate(const StageBuf s, const h261b_session_dev_t &S, int mbx, int mby,
                                                 int lane, me_gpu_mb_t &res, int8_t &s1x, int8_t &s1y)
 {
     const int bx = mbx * 16, by = mby * 16;
@@ -416,7 +445,7 @@ __device__ __forceinline__ void motion_estimate(const StageBuf &s, const h261b_s
     int32_t d[16], di[16];
 #pragma unroll
     for (int iy = 0; iy < 4; iy++) {
-        const uint32_t cw = s.cur[(sy * 4 + iy) * 4 + sx];
+        const uint32_t cw = *s.cur(sy * 4 + iy, sx);
 #pragma unroll
         for (int ix = 0; ix < 4; ix++) {
             const int c = (int)((cw >> (8 * ix)) & 0xFFu);
@@ -485,7 +514,7 @@ __device__ __forceinline__ int hfilt(uint2 v, int c)
  * column).  Adds the block-summed |coefficient| of column (lane & 7) to
  * colsum[v] and returns this pass's CBP bits. */
 template <int FMAD>
-__device__ __forceinline__ uint32_t encdec_pass(float (*tb)[72], const StageBuf &s, const h261b_session_dev_t &S,
+__device__ __forceinline__ uint32_t encdec_pass(float (*tb)[72], const StageBuf s, const h261b_session_dev_t &S,
                                                 int mb, int mbx, int mby, const MbDecision &m, int quant,
                                                 bool luma_pass, int lane, int32_t colsum[8], uint32_t &ssd)
 {
@@ -504,8 +533,8 @@ __device__ __forceinline__ uint32_t encdec_pass(float (*tb)[72], const StageBuf 
     for (int i = 0; i < 8; i++)
         pred[i] = 0;
     if (active) {
-        const uint2 cw = luma_pass ? *reinterpret_cast<const uint2 *>(&s.cur[(by8 + r) * 4 + (bx8 >> 2)])
-                                   : *reinterpret_cast<const uint2 *>(&s.curc[b - 4][2 * r]);
+        const uint2 cw = luma_pass ? *reinterpret_cast<const uint2 *>(s.cur(by8 + r, bx8 >> 2))
+                                   : *reinterpret_cast<const uint2 *>(s.curc(8 * (b - 4) + r));
         if (intra) {
 #pragma unroll
             for (int i = 0; i < 8; i++)
@@ -716,8 +745,8 @@ __device__ __forceinline__ uint32_t encdec_pass(float (*tb)[72], const StageBuf 
         if (S.ssd_out) {
             /* squared error of this row against the source, for the
              * picture's PSNR (h261_main.c:38-91) */
-            const uint2 cw = luma_pass ? *reinterpret_cast<const uint2 *>(&s.cur[(by8 + r) * 4 + (bx8 >> 2)])
-                                       : *reinterpret_cast<const uint2 *>(&s.curc[b - 4][2 * r]);
+            const uint2 cw = luma_pass ? *reinterpret_cast<const uint2 *>(s.cur(by8 + r, bx8 >> 2))
+                                       : *reinterpret_cast<const uint2 *>(s.curc(8 * (b - 4) + r));
             const uint2 rw = make_uint2(lo, hi);
             uint32_t e = 0;
 #pragma unroll
@@ -781,10 +810,15 @@ __device__ __forceinline__ void publish_run(const h261b_session_dev_t &S, int t,
     }
 }
 
+/* resident CTAs of 256 threads the register allocation must allow per SM */
+#ifndef H261B_STEP_MIN_BLOCKS
+#define H261B_STEP_MIN_BLOCKS 2
+#endif
+
 template <int FMAD>
-__global__ void __launch_bounds__(256) step_kernel(const h261b_session_dev_t *__restrict__ sessions,
-                                                   const uint32_t *__restrict__ work, int32_t n_work, int32_t chunk,
-                                                   int32_t phases)
+__global__ void __launch_bounds__(256, H261B_STEP_MIN_BLOCKS)
+    step_kernel(const h261b_session_dev_t *__restrict__ sessions, const uint32_t *__restrict__ work, int32_t n_work,
+                int32_t chunk, int32_t phases)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -800,7 +834,7 @@ __global__ void __launch_bounds__(256) step_kernel(const h261b_session_dev_t *__
         const uint32_t item = work[begin];
         const h261b_session_dev_t &S = sessions[item >> 12];
         const int mb = (int)(item & 0xFFFu), mby = mb / S.mbw;
-        stage_mb(sm.buf[0], S, mb - mby * S.mbw, mby, lane);
+        stage_mb(sm, 0, S, mb - mby * S.mbw, mby, lane);
         cp_async_commit();
     }
 
@@ -816,7 +850,7 @@ __global__ void __launch_bounds__(256) step_kernel(const h261b_session_dev_t *__
             const uint32_t nitem = work[g + 1];
             const h261b_session_dev_t &N = sessions[nitem >> 12];
             const int nmb = (int)(nitem & 0xFFFu), nmby = nmb / N.mbw;
-            stage_mb(sm.buf[cur ^ 1], N, nmb - nmby * N.mbw, nmby, lane);
+            stage_mb(sm, cur ^ 1, N, nmb - nmby * N.mbw, nmby, lane);
             cp_async_commit();
             cp_async_wait<1>();
         } else {
@@ -829,7 +863,7 @@ __global__ void __launch_bounds__(256) step_kernel(const h261b_session_dev_t *__
         const h261b_session_dev_t &S = sessions[sidx];
         const int mb = (int)(item & 0xFFFu);
         const int mby = mb / S.mbw, mbx = mb - mby * S.mbw;
-        const StageBuf &b = sm.buf[cur];
+        const StageBuf b = stage_view(sm, cur);
         const bool do_me = (phases & H261B_PHASE_ME) && !S.skip_search;
 
         me_gpu_mb_t me;
@@ -856,7 +890,7 @@ __global__ void __launch_bounds__(256) step_kernel(const h261b_session_dev_t *__
                 const int sb = lane & 15;
 #pragma unroll
                 for (int iy = 0; iy < 4; iy++) {
-                    const uint32_t cw = b.cur[((sb >> 2) * 4 + iy) * 4 + (sb & 3)];
+                    const uint32_t cw = *b.cur((sb >> 2) * 4 + iy, sb & 3);
 #pragma unroll
                     for (int ix = 0; ix < 4; ix++)
                         d[iy * 4 + ix] = (int32_t)((cw >> (8 * ix)) & 0xFFu);
