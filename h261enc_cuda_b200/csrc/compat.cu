@@ -302,7 +302,8 @@ extern "C" void h261_gpu_device_me(me_gpu_t *s)
     d.frame_type = H261B_FRAME_TYPE_INTER;
     d.me_out = s->prgs_macroblocks_device;
     CK(where, cudaMemcpyAsync(g.desc_dev, &d, sizeof(d), cudaMemcpyHostToDevice, g.stream));
-    int rc = h261b_launch_step(g.desc_dev, g.work_dev, n, H261B_PHASE_ME | (g.fmad ? 0x100 : 0), 4, 0, g.stream);
+    int rc = h261b_launch_step(g.desc_dev, g.work_dev, n, H261B_PHASE_ME | (g.fmad ? 0x100 : 0), 4, 0, nullptr,
+                               g.stream);
     if (rc) {
         fail(where, (cudaError_t)rc);
         return;
@@ -481,7 +482,7 @@ extern "C" void h261_gpu_device_encode_macroblocks(h261_context_t *ctx)
     d.frame_type = ctx->s_picture.i_frame_type;
     CK(where, cudaMemcpyAsync(g.desc_dev, &d, sizeof(d), cudaMemcpyHostToDevice, g.stream));
     int rc = h261b_launch_step(g.desc_dev, g.work_dev, n, H261B_PHASE_ENCDEC | (g.fmad ? 0x100 : 0), 4, 0,
-                               g.stream);
+                               nullptr, g.stream);
     if (rc) {
         fail(where, (cudaError_t)rc);
         return;

@@ -261,6 +261,8 @@ struct h261b_engine_s {
      * start (the previous step's encode is done), results downloaded */
     cudaEvent_t t_begin[2] = { nullptr, nullptr }, t_h2d[2] = { nullptr, nullptr };
     cudaEvent_t t_ready[2] = { nullptr, nullptr }, t_end[2] = { nullptr, nullptr };
+    /* the encode launches' work counters, two per stream (h261b_launch_step) */
+    int32_t *sched_dev = nullptr;
     bool step_bits_ran[2] = { false, false };
     bool in_flight[2] = { false, false };
     int64_t step_mbs[2] = { 0, 0 };   /* MB records of the step in each arena */
@@ -414,6 +416,8 @@ extern "C" int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engin
              cudaEventCreate(&e->t_h2d[p]) == cudaSuccess && cudaEventCreate(&e->t_ready[p]) == cudaSuccess &&
              cudaEventCreate(&e->t_end[p]) == cudaSuccess;
     }
+    ok = ok && cudaMalloc(&e->sched_dev, 4 * sizeof(int32_t)) == cudaSuccess &&
+         cudaMemset(e->sched_dev, 0, 4 * sizeof(int32_t)) == cudaSuccess;
     if (!ok) {
         set_error("h261b_engine_create: device setup failed: %s", cudaGetErrorString(cudaGetLastError()));
         h261b_engine_destroy(e);
@@ -477,6 +481,8 @@ extern "C" int h261b_engine_destroy(h261b_engine_t *e)
         if (e->stream[p])
             cudaStreamDestroy(e->stream[p]);
     }
+    if (e->sched_dev)
+        cudaFree(e->sched_dev);
     delete e;
     return H261B_OK;
 }
@@ -1027,7 +1033,8 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
             H261B_CUDA_TRY(cudaStreamWaitEvent(st, e->kernel_done[p ^ 1], wf));
         H261B_CUDA_TRY(cudaEventRecordWithFlags(e->t_ready[p], st, rf));
         H261B_CUDA_TRY(cudaEventRecordWithFlags(e->k_start[p], st, rf));
-        int lr = h261b_launch_step(desc_dev, work_dev, n_work, phases, warps, ctas, st);
+        int32_t *sched = e->sched_dev + 2 * p;
+        int lr = h261b_launch_step(desc_dev, work_dev, n_work, phases, warps, ctas, sched, st);
         if (lr == 0 && n_rc) {
             /* rate-controlled sessions: the picture QUANT from this
              * picture's costs and the previous picture's size (written by
@@ -1037,7 +1044,7 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
             lr = h261b_launch_ratectrl(desc_dev, (int32_t)n, st);
             if (lr == 0)
                 lr = h261b_launch_step(desc_dev, work_dev + rc_begin, n_work - rc_begin,
-                                       H261B_PHASE_ENCDEC | (e->cfg.fmad ? 0x100 : 0), warps, ctas, st);
+                                       H261B_PHASE_ENCDEC | (e->cfg.fmad ? 0x100 : 0), warps, ctas, sched, st);
         }
         if (lr != 0) {
             set_error("step launch failed: %s", cudaGetErrorString((cudaError_t)lr));

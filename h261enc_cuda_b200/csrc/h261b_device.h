@@ -137,10 +137,13 @@ typedef struct {
 #ifdef __cplusplus
 extern "C" {
 #endif
-/* host-side launchers (kernels.cu); return a cudaError_t value */
+/* host-side launchers (kernels.cu); return a cudaError_t value.
+ * h261b_launch_step: sched_dev, when not null, is two int32 counters, zero
+ * before the first launch and left zero by each, that balance the launch's
+ * tail; one launch at a time may use them (null: static runs only). */
 int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const uint32_t *work_dev,
                       int32_t n_work, int32_t phases, int32_t warps_per_cta, int32_t max_ctas,
-                      void *stream);
+                      int32_t *sched_dev, void *stream);
 int h261b_set_quant_table(void);
 /* the picture QUANT of every session with rc (one thread per session) */
 int h261b_launch_ratectrl(h261b_session_dev_t *sessions_dev, int32_t n_sessions, void *stream);

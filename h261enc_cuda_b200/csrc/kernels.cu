@@ -41,6 +41,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "h261b_device.h"
@@ -82,7 +83,13 @@ struct StageBuf {
 
 __device__ __forceinline__ StageBuf stage_view(const WarpSmem &w, int k) { return StageBuf{ w.buf + 16 * k }; }
 
-__constant__ int8_t c_stage1[11] = { -14, -11, -8, -5, -2, 0, 2, 5, 8, 11, 14 };
+/* the coarse grid's offsets { -14, -11, -8, -5, -2, 0, 2, 5, 8, 11, 14 }
+ * (megpu_kernels.cuh:27-166), by arithmetic: lanes index it at 11 places
+ * at once, which a constant-memory table would serve one address at a time */
+__device__ __forceinline__ int stage1_offset(int t)
+{
+    return 3 * t - 14 - (t == 5 ? 1 : 0) - (t > 5 ? 2 : 0);
+}
 /* float tables initialised from double literals like the reference's */
 __constant__ float c_fwd_post[8] = { 1.0, 0.720960, 0.765367, 0.850430, 1.0, 1.272759, 1.847759, 3.624510 };
 __constant__ float c_inv_pre[8] = { 1.0, 1.387040, 1.306563, 1.175876, 1.0, 0.785695, 0.541196, 0.275899 };
@@ -398,7 +405,7 @@ __device__ __forceinline__ void motion_estimate(const StageBuf s, const h261b_se
             const int c1 = c + 32;
             const bool has1 = c1 < 121;
             const int ty0 = c / 11, tx0 = c - ty0 * 11, ty1 = (has1 ? c1 : c) / 11, tx1 = (has1 ? c1 : c) - ty1 * 11;
-            const int x0 = c_stage1[tx0], y0 = c_stage1[ty0], x1 = c_stage1[tx1], y1 = c_stage1[ty1];
+            const int x0 = stage1_offset(tx0), y0 = stage1_offset(ty0), x1 = stage1_offset(tx1), y1 = stage1_offset(ty1);
             const bool o0 = x0 >= lminx && x0 <= lmaxx && y0 >= lminy && y0 <= lmaxy;
             const bool o1 = has1 && x1 >= lminx && x1 <= lmaxx && y1 >= lminy && y1 <= lmaxy;
             uint32_t s0, s1;
@@ -408,7 +415,7 @@ __device__ __forceinline__ void motion_estimate(const StageBuf s, const h261b_se
                 best = min(best, ((o1 ? s1 : 65535u) << 10) | zorder(tx1, ty1));
         }
         best = __reduce_min_sync(FULL, best) & 1023u; /* Z-order index only */
-        const int v1x = c_stage1[compact8(best)], v1y = c_stage1[compact8(best >> 1)];
+        const int v1x = stage1_offset((int)compact8(best)), v1y = stage1_offset((int)compact8(best >> 1));
         s1x = (int8_t)v1x;
         s1y = (int8_t)v1y;
         best = FULL;
@@ -442,6 +449,18 @@ __device__ __forceinline__ void motion_estimate(const StageBuf s, const h261b_se
 #pragma unroll
     for (int k = 0; k < 6; k++)
         rr[k] = win8(s, min(max(wr0 - 1 + k, 0), WIN_ROWS - 1), wc0 - 1);
+    /* the 3x3 filter, separable: horizontal [1 2 1] sums of rows R = 0..5
+     * at columns C = 1..4, then vertical [1 2 1] over them.  Pixel (ix, iy)
+     * of the sub-block sits at (lx, ly) = ((sx & 1) * 4 + ix, (sy & 1) * 4
+     * + iy) of its 8x8 block; only the block's interior (1..6) is filtered */
+    int32_t hs[6][4];
+#pragma unroll
+    for (int R = 0; R < 6; R++) {
+#pragma unroll
+        for (int C = 1; C <= 4; C++)
+            hs[R][C - 1] = byte8(rr[R], C - 1) + 2 * byte8(rr[R], C) + byte8(rr[R], C + 1);
+    }
+    const uint32_t xin = (sx & 1) ? 0x7u : 0xEu, yin = (sy & 1) ? 0x7u : 0xEu; /* interior ix / iy bits */
     int32_t d[16], di[16];
 #pragma unroll
     for (int iy = 0; iy < 4; iy++) {
@@ -449,16 +468,9 @@ __device__ __forceinline__ void motion_estimate(const StageBuf s, const h261b_se
 #pragma unroll
         for (int ix = 0; ix < 4; ix++) {
             const int c = (int)((cw >> (8 * ix)) & 0xFFu);
-            const int lx = (sx & 1) * 4 + ix, ly = (sy & 1) * 4 + iy;
-            const int R = iy + 1, C = ix + 1;
-            int p;
-            if (filt && lx >= 1 && lx <= 6 && ly >= 1 && ly <= 6) {
-                p = (byte8(rr[R - 1], C - 1) + 2 * byte8(rr[R - 1], C) + byte8(rr[R - 1], C + 1) +
-                     2 * byte8(rr[R], C - 1) + 4 * byte8(rr[R], C) + 2 * byte8(rr[R], C + 1) +
-                     byte8(rr[R + 1], C - 1) + 2 * byte8(rr[R + 1], C) + byte8(rr[R + 1], C + 1) + 8) >> 4;
-            } else {
-                p = byte8(rr[R], C);
-            }
+            const int f = (hs[iy][ix] + 2 * hs[iy + 1][ix] + hs[iy + 2][ix] + 8) >> 4;
+            const bool use_f = filt && ((xin >> ix) & (yin >> iy) & 1u);
+            const int p = use_f ? f : byte8(rr[iy + 1], ix + 1);
             d[iy * 4 + ix] = c - p;
             di[iy * 4 + ix] = c;
         }
@@ -528,10 +540,8 @@ __device__ __forceinline__ uint32_t encdec_pass(float (*tb)[72], const StageBuf 
     /* ---- prediction and residual of row r (mbgpu_kernels.cuh:59-166):
      * the source row and up to three reference rows as 8-byte vectors */
     const int bx8 = luma_pass ? (b & 1) * 8 : 0, by8 = luma_pass ? (b >> 1) * 8 : 0;
-    int32_t pred[8], res[8];
-#pragma unroll
-    for (int i = 0; i < 8; i++)
-        pred[i] = 0;
+    int32_t res[8];
+    uint32_t pred_lo = 0, pred_hi = 0;   /* the row's prediction, one byte a pixel */
     if (active) {
         const uint2 cw = luma_pass ? *reinterpret_cast<const uint2 *>(s.cur(by8 + r, bx8 >> 2))
                                    : *reinterpret_cast<const uint2 *>(s.curc(8 * (b - 4) + r));
@@ -568,7 +578,10 @@ __device__ __forceinline__ uint32_t encdec_pass(float (*tb)[72], const StageBuf 
                 } else {
                     p = byte8(rb, i);
                 }
-                pred[i] = p;
+                if (i < 4)
+                    pred_lo |= (uint32_t)p << (8 * i);
+                else
+                    pred_hi |= (uint32_t)p << (8 * (i - 4));
                 res[i] = byte8(cw, i) - p;
             }
         }
@@ -599,7 +612,7 @@ __device__ __forceinline__ uint32_t encdec_pass(float (*tb)[72], const StageBuf 
             q[k] = tb[slot][k * 9 + c];
         fdct_butterfly<FMAD>(q[0] + q[7], q[1] + q[6], q[2] + q[5], q[3] + q[4], q[3] - q[4], q[2] - q[5],
                              q[1] - q[6], q[0] - q[7], o);
-        const float cs = dmulf(c_fwd_post[c], 0.125);
+        const float cs = __fmul_rn(c_fwd_post[c], 0.125f); /* = dmulf(.., 0.125): a power-of-two scaling is exact */
         const float inv = c_inv_quant[quant];
         /* this column's eight offsets, UInt16, one 16-byte load */
         const uint4 ow = *reinterpret_cast<const uint4 *>(&S.dn->offset[t][c][0]);
@@ -692,7 +705,7 @@ __device__ __forceinline__ uint32_t encdec_pass(float (*tb)[72], const StageBuf 
             float P[8], cs[8], tt[8], o[8];
 #pragma unroll
             for (int k = 0; k < 8; k++) {
-                cs[k] = dmulf(c_inv_pre[k], 0.125);
+                cs[k] = __fmul_rn(c_inv_pre[k], 0.125f); /* exact, as dmulf(.., 0.125) */
                 P[k] = __fmul_rn(col[k], c_inv_pre[c]);
                 tt[k] = __fmul_rn(P[k], cs[k]);
             }
@@ -730,7 +743,8 @@ __device__ __forceinline__ uint32_t encdec_pass(float (*tb)[72], const StageBuf 
         uint32_t lo = 0, hi = 0;
 #pragma unroll
         for (int i = 0; i < 8; i++) {
-            const int32_t v = min(255, max(0, intra ? out[i] : out[i] + pred[i]));
+            const int32_t pi = (int32_t)(((i < 4 ? pred_lo : pred_hi) >> (8 * (i & 3))) & 0xFFu);
+            const int32_t v = min(255, max(0, out[i] + pi));
             if (i < 4)
                 lo |= (uint32_t)v << (8 * i);
             else
@@ -815,28 +829,53 @@ __device__ __forceinline__ void publish_run(const h261b_session_dev_t &S, int t,
 #define H261B_STEP_MIN_BLOCKS 2
 #endif
 
+/* Work items are handed out in two parts.  Warp w first takes the static
+ * run [w * chunk, (w + 1) * chunk) of the first total_warps * chunk items
+ * (consecutive MBs of mostly one session: neighbouring windows hit in L1
+ * and the denoise statistics publish once per run).  With a scheduler
+ * (sched != nullptr, two zeroed counters) the remaining items are then
+ * drawn one at a time from sched[0], so that warps which met cheaper MBs
+ * take more of the tail; every warp makes exactly one fetch past the end,
+ * and the last warp to finish (sched[1]) zeroes both counters for the next
+ * launch.  Without a scheduler the static runs cover every item. */
 template <int FMAD>
 __global__ void __launch_bounds__(256, H261B_STEP_MIN_BLOCKS)
     step_kernel(const h261b_session_dev_t *__restrict__ sessions, const uint32_t *__restrict__ work, int32_t n_work,
-                int32_t chunk, int32_t phases)
+                int32_t chunk, int32_t phases, int32_t *sched)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     WarpSmem &sm = reinterpret_cast<WarpSmem *>(smem_raw)[warp];
     const int warps = blockDim.x >> 5;
-    const int begin = (blockIdx.x * warps + warp) * chunk;
-    const int end = min(begin + chunk, n_work);
-    if (begin >= end)
-        return;
+    const int total_warps = gridDim.x * warps;
+    const int n_static = sched ? min(n_work, total_warps * chunk) : n_work;
+    int static_next = (blockIdx.x * warps + warp) * chunk;
+    const int static_end = min(static_next + chunk, n_static);
+    /* the warp's next work item (n_work when it has none left): a static
+     * index, or a draw from the scheduler while the static run lasts */
+    auto next_item = [&]() -> int {
+        if (static_next < static_end)
+            return static_next++;
+        if (!sched)
+            return n_work;
+        int v = 0;
+        if (lane == 0)
+            v = n_static + atomicAdd(&sched[0], 1);
+        return min(__shfl_sync(FULL, v, 0), n_work);
+    };
     const bool want_enc = (phases & H261B_PHASE_ENCDEC) != 0;
 
-    {
-        const uint32_t item = work[begin];
+    int g = next_item();
+    uint32_t item = g < n_work ? work[g] : 0u;
+    if (g < n_work) {
         const h261b_session_dev_t &S = sessions[item >> 12];
         const int mb = (int)(item & 0xFFFu), mby = mb / S.mbw;
         stage_mb(sm, 0, S, mb - mby * S.mbw, mby, lane);
         cp_async_commit();
     }
+    /* the item after g, known one MB ahead of its staging */
+    int gn = g < n_work ? next_item() : n_work;
+    uint32_t nitem = gn < n_work ? work[gn] : 0u;
 
     int run_s = -1, run_t = 0, run_n = 0;
     int32_t colsum[8];
@@ -844,10 +883,10 @@ __global__ void __launch_bounds__(256, H261B_STEP_MIN_BLOCKS)
     for (int v = 0; v < 8; v++)
         colsum[v] = 0;
 
-    for (int g = begin; g < end; g++) {
-        const int cur = (g - begin) & 1;
-        if (g + 1 < end) {
-            const uint32_t nitem = work[g + 1];
+    for (int cur = 0; g < n_work; cur ^= 1) {
+        const int gnn = gn < n_work ? next_item() : n_work;
+        const uint32_t nnitem = gnn < n_work ? work[gnn] : 0u;
+        if (gn < n_work) {
             const h261b_session_dev_t &N = sessions[nitem >> 12];
             const int nmb = (int)(nitem & 0xFFFu), nmby = nmb / N.mbw;
             stage_mb(sm, cur ^ 1, N, nmb - nmby * N.mbw, nmby, lane);
@@ -858,7 +897,6 @@ __global__ void __launch_bounds__(256, H261B_STEP_MIN_BLOCKS)
         }
         __syncwarp();
 
-        const uint32_t item = work[g];
         const int sidx = (int)(item >> 12);
         const h261b_session_dev_t &S = sessions[sidx];
         const int mb = (int)(item & 0xFFFu);
@@ -984,9 +1022,20 @@ __global__ void __launch_bounds__(256, H261B_STEP_MIN_BLOCKS)
             }
         }
         __syncwarp(); /* this buffer may be refilled from the next iteration on */
+        g = gn;
+        item = nitem;
+        gn = gnn;
+        nitem = nnitem;
     }
     if (want_enc && run_n > 0)
         publish_run(sessions[run_s], run_t, run_n, colsum, lane);
+    if (sched && lane == 0) {
+        __threadfence();
+        if (atomicAdd(&sched[1], 1) == total_warps - 1) {
+            atomicExch(&sched[0], 0);
+            atomicExch(&sched[1], 0);
+        }
+    }
 }
 
 } // namespace
@@ -1004,7 +1053,7 @@ extern "C" int h261b_set_quant_table(void)
 
 extern "C" int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const uint32_t *work_dev,
                                  int32_t n_work, int32_t phases, int32_t warps_per_cta, int32_t max_ctas,
-                                 void *stream)
+                                 int32_t *sched_dev, void *stream)
 {
     if (n_work <= 0)
         return 0;
@@ -1014,7 +1063,6 @@ extern "C" int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const 
     const int ph = phases & 0xFF;
     const int threads = warps_per_cta * 32;
     const size_t smem = sizeof(WarpSmem) * (size_t)warps_per_cta;
-    /* one wave of resident CTAs, each warp a contiguous run of work items */
     static std::mutex mu;
     static int sms[64], resident[64][2][9];
     int dev = 0;
@@ -1043,15 +1091,30 @@ extern "C" int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const 
         per_sm = r;
         nsm = sms[dev];
     }
+    /* one wave of resident CTAs */
     int ctas = max_ctas > 0 ? max_ctas : nsm * per_sm;
-    const long long total_warps = (long long)ctas * warps_per_cta;
-    const int chunk = (int)((n_work + total_warps - 1) / total_warps);
-    ctas = (n_work + chunk * warps_per_cta - 1) / (chunk * warps_per_cta);
+    int chunk;
+    if (sched_dev) {
+        /* static runs of all but about kTailPerWarp items per warp, the rest
+         * drawn from the scheduler */
+#ifndef H261B_TAIL_PER_WARP
+#define H261B_TAIL_PER_WARP 2
+#endif
+        constexpr int kTailPerWarp = H261B_TAIL_PER_WARP;
+        ctas = (int)std::min<long long>(ctas, (n_work + warps_per_cta - 1) / warps_per_cta);
+        const long long total_warps = (long long)ctas * warps_per_cta;
+        chunk = (int)std::max<long long>(0, n_work / total_warps - kTailPerWarp);
+    } else {
+        /* contiguous runs covering every item */
+        const long long total_warps = (long long)ctas * warps_per_cta;
+        chunk = (int)((n_work + total_warps - 1) / total_warps);
+        ctas = (n_work + chunk * warps_per_cta - 1) / (chunk * warps_per_cta);
+    }
     cudaStream_t st = (cudaStream_t)stream;
     if (fmad)
-        step_kernel<1><<<ctas, threads, smem, st>>>(sessions_dev, work_dev, n_work, chunk, ph);
+        step_kernel<1><<<ctas, threads, smem, st>>>(sessions_dev, work_dev, n_work, chunk, ph, sched_dev);
     else
-        step_kernel<0><<<ctas, threads, smem, st>>>(sessions_dev, work_dev, n_work, chunk, ph);
+        step_kernel<0><<<ctas, threads, smem, st>>>(sessions_dev, work_dev, n_work, chunk, ph, sched_dev);
     return (int)cudaGetLastError();
 }
 

@@ -158,7 +158,8 @@ extern "C" int h261b_encode_picture_noalloc(const h261b_noalloc_picture_t *p, vo
     H261B_CUDA_TRY(cudaMemcpyAsync(scratch, &d, sizeof(d), cudaMemcpyHostToDevice, st));
     const int phases = H261B_PHASE_ME | H261B_PHASE_MD | H261B_PHASE_ENCDEC | (p->fmad ? 0x100 : 0);
     const int lr = h261b_launch_step((const h261b_session_dev_t *)scratch,
-                                     (const uint32_t *)((const uint8_t *)scratch + kDescBytes), nmb, phases, 4, 0, st);
+                                     (const uint32_t *)((const uint8_t *)scratch + kDescBytes), nmb, phases, 4, 0,
+                                     nullptr, st);
     if (lr != 0) {
         set_error("h261b_encode_picture_noalloc: launch failed: %s", cudaGetErrorString((cudaError_t)lr));
         return H261B_ERR_CUDA;
