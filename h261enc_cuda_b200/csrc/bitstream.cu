@@ -29,6 +29,12 @@
  *   copy    the picture into the host arena (mapped pinned memory), at
  *           the offset layout drew with one atomic, split over several
  *           CTAs per picture.
+ *
+ * Layout, pack and copy are programmatic dependent launches: each kernel
+ * of the chain lets the next one launch as soon as its own CTAs are
+ * running, and the next one's CTAs wait (griddepcontrol.wait) for the
+ * whole previous grid and its memory before they read what it wrote, so
+ * a launch's latency overlaps the kernel before it.
  */
 #include <cuda_runtime.h>
 #include <stddef.h>
@@ -36,8 +42,20 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 #include "h261b_device.h"
+
+namespace {
+
+/* programmatic dependent launch: allow the next kernel in the stream to
+ * launch now / wait until the previous kernel has completed and its
+ * writes are visible (both no-ops for a kernel launched without the
+ * attribute) */
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+} // namespace
 #include "ratectrl_dev.h"
 #include "vlc_tables.h"
 
@@ -187,15 +205,12 @@ __global__ void __launch_bounds__(VLC_THREADS) codes_kernel(const h261b_session_
                                                             const uint32_t *work, int32_t n_work)
 {
     __shared__ CodesSmem sm;
+    pdl_launch_dependents();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int i = tid; i < 27 * 16; i += VLC_THREADS)
         (&sm.tc[0][0])[i] = (&c_vlc_tcoeff[0][0])[i];
-    if (tid < 64) {
-        for (int v = 0; v < 8; v++)
-            for (int u = 0; u < 8; u++)
-                if (zigzag_index(v, u) == tid)
-                    sm.zz_cm[tid] = (uint8_t)(u * 8 + v);
-    }
+    if (tid < 64)
+        sm.zz_cm[tid] = c_zigzag_cm.cm[tid];
     uint32_t *stage = sm.stage[warp];
     for (int i = lane; i < MB_WORDS; i += 32)
         stage[i] = 0u;
@@ -330,9 +345,11 @@ constexpr int COPY_SPLIT = 8;
 __global__ void __launch_bounds__(LAYOUT_THREADS) layout_kernel(const h261b_session_dev_t *sessions,
                                                                 h261b_step_dev_t *step, int64_t host_cap)
 {
+    pdl_launch_dependents();
     const h261b_session_dev_t &S = sessions[blockIdx.x];
     if (!S.bits_out)
         return;
+    pdl_wait();   /* the codes kernel's MB sizes */
     __shared__ int32_t rel[396];       /* MB position within its GOB */
     __shared__ int32_t gob_bits[12];
     __shared__ int64_t gob_start[13];
@@ -459,9 +476,11 @@ __global__ void __launch_bounds__(LAYOUT_THREADS) layout_kernel(const h261b_sess
 __global__ void __launch_bounds__(VLC_THREADS) pack_kernel(const h261b_session_dev_t *sessions,
                                                            const uint32_t *work, int32_t n_work)
 {
+    pdl_launch_dependents();
     const int lane = threadIdx.x & 31;
     int lo, hi;
     warp_range(n_work, lo, hi);
+    pdl_wait();   /* the layout kernel's positions */
     for (int w = lo; w < hi; w++) {
         const uint32_t item = work[w];
         const h261b_session_dev_t &S = sessions[item >> 12];
@@ -553,6 +572,7 @@ __global__ void __launch_bounds__(VLC_THREADS) copy_kernel(const h261b_session_d
     const h261b_session_dev_t &S = sessions[blockIdx.x];
     if (!S.bits_out)
         return;
+    pdl_wait();   /* the packed picture */
     const int total = S.vlc_total[0];
     const int64_t words = ((int64_t)(total + 127) / 128) * 4;
     const int st = (total < 0 || words * 4 > S.bits_cap) ? H261B_BITS_OVERFLOW : S.vlc_total[1];
@@ -596,18 +616,72 @@ extern "C" h261b_bits_layout_t h261b_bits_layout(int32_t w, int32_t h)
 
 extern "C" int64_t h261b_bits_slot_bytes(int32_t w, int32_t h) { return h261b_bits_layout(w, h).bytes; }
 
+/* CTAs of the codes and pack kernels resident per SM, per device */
+static cudaError_t resident_ctas(const void *codes, const void *pack, int *codes_res, int *pack_res)
+{
+    static std::mutex mu;
+    static int cached[64][2];
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess)
+        return err;
+    if (dev < 0 || dev >= 64)
+        return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(mu);
+    int *c = cached[dev];
+    if (!c[0]) {
+        if ((err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c[0], codes, VLC_THREADS, 0)) != cudaSuccess ||
+            (err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c[1], pack, VLC_THREADS, 0)) != cudaSuccess)
+            return err;
+        c[0] = std::max(c[0], 1);
+        c[1] = std::max(c[1], 1);
+    }
+    *codes_res = c[0];
+    *pack_res = c[1];
+    return cudaSuccess;
+}
+
+/* a launch that may begin while the kernel before it in the stream runs */
+template <typename... Params, typename... Args>
+static cudaError_t launch_dependent(void (*kernel)(Params...), dim3 grid, dim3 block, cudaStream_t st,
+                                    Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 extern "C" int h261b_launch_bitstream(h261b_session_dev_t *sessions_dev, int32_t n_sessions, const uint32_t *work_dev,
                                       int32_t n_work, h261b_step_dev_t *step, uint8_t *host_arena_dev,
                                       int64_t host_cap, int32_t sm_count, void *stream, void *layout_done_event)
 {
     if (n_work <= 0 || n_sessions <= 0)
         return 0;
-    /* two MBs per warp, up to eight CTAs per SM: latency-bound kernels want
-     * every warp slot they can get */
-    const int ctas = (int)std::min<int64_t>((n_work + 2 * VLC_WARPS - 1) / (2 * VLC_WARPS), (int64_t)sm_count * 8);
+    /* at least two MBs per warp, and no more CTAs than are resident at once
+     * (latency-bound kernels want every warp slot they can get, but a
+     * second, partial wave would only add a tail) */
+    int codes_res = 0, pack_res = 0;
+    cudaError_t err = resident_ctas((const void *)codes_kernel, (const void *)pack_kernel, &codes_res, &pack_res);
+    if (err != cudaSuccess)
+        return (int)err;
+    const int64_t want = (n_work + 2 * VLC_WARPS - 1) / (2 * VLC_WARPS);
+    const int codes_ctas = (int)std::min<int64_t>(want, (int64_t)sm_count * codes_res);
+    const int ctas = (int)std::min<int64_t>(want, (int64_t)sm_count * pack_res);
     cudaStream_t st = (cudaStream_t)stream;
-    codes_kernel<<<ctas, VLC_THREADS, 0, st>>>(sessions_dev, work_dev, n_work);
-    layout_kernel<<<n_sessions, LAYOUT_THREADS, 0, st>>>(sessions_dev, step, host_arena_dev ? host_cap : 0);
+    codes_kernel<<<codes_ctas, VLC_THREADS, 0, st>>>(sessions_dev, work_dev, n_work);
+    err = launch_dependent(layout_kernel, dim3(n_sessions), dim3(LAYOUT_THREADS), st,
+                                       (const h261b_session_dev_t *)sessions_dev, step,
+                                       (int64_t)(host_arena_dev ? host_cap : 0));
+    if (err != cudaSuccess)
+        return (int)err;
     if (layout_done_event) {
         /* the next step's rate control reads what the layout updated */
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -619,7 +693,13 @@ extern "C" int h261b_launch_bitstream(h261b_session_dev_t *sessions_dev, int32_t
         if (err != cudaSuccess)
             return (int)err;
     }
-    pack_kernel<<<ctas, VLC_THREADS, 0, st>>>(sessions_dev, work_dev, n_work);
-    copy_kernel<<<dim3(n_sessions, COPY_SPLIT), VLC_THREADS, 0, st>>>(sessions_dev, host_arena_dev);
+    err = launch_dependent(pack_kernel, dim3(ctas), dim3(VLC_THREADS), st, (const h261b_session_dev_t *)sessions_dev,
+                           work_dev, n_work);
+    if (err != cudaSuccess)
+        return (int)err;
+    err = launch_dependent(copy_kernel, dim3(n_sessions, COPY_SPLIT), dim3(VLC_THREADS), st,
+                           (const h261b_session_dev_t *)sessions_dev, host_arena_dev);
+    if (err != cudaSuccess)
+        return (int)err;
     return (int)cudaGetLastError();
 }

@@ -1056,7 +1056,7 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
         if (n_bits) {
             lr = h261b_launch_bitstream(desc_dev, (int32_t)n, work_dev, n_work, (h261b_step_dev_t *)dm.dev,
                                         e->bits[p].dev, (int64_t)e->bits[p].cap, e->sm_count, st,
-                                        (void *)e->layout_done[p]);
+                                        n_rc ? (void *)e->layout_done[p] : nullptr);
             if (lr != 0) {
                 set_error("bitstream launch failed: %s", cudaGetErrorString((cudaError_t)lr));
                 return H261B_ERR_CUDA;

@@ -76,13 +76,26 @@ static __device__ __constant__ uint8_t c_vlc_mtype_len[10] = { 4, 7, 1, 5, 9, 8,
  * diagonal d = u + v starts at d(d+1)/2 (or 64 - (15-d)(16-d)/2 past the
  * main anti-diagonal); odd diagonals run with increasing v, even ones with
  * decreasing v -- the transmission order of H.261 */
-__device__ __forceinline__ int zigzag_index(int v, int u)
+__host__ __device__ constexpr int zigzag_index(int v, int u)
 {
-    const int d = u + v;
-    const int start = d < 8 ? (d * (d + 1)) >> 1 : 64 - (((15 - d) * (16 - d)) >> 1);
-    const int vmin = d < 8 ? 0 : d - 7, vmax = d < 8 ? d : 7;
-    return start + ((d & 1) ? v - vmin : vmax - v);
+    return (u + v < 8 ? ((u + v) * (u + v + 1)) >> 1 : 64 - (((15 - u - v) * (16 - u - v)) >> 1)) +
+           (((u + v) & 1) ? v - (u + v < 8 ? 0 : u + v - 7) : (u + v < 8 ? u + v : 7) - v);
 }
+
+/* column-major index (u * 8 + v) of the k-th coefficient sent, generated
+ * from zigzag_index at compile time */
+struct ZigzagTable {
+    uint8_t cm[64];
+};
+__host__ __device__ constexpr ZigzagTable make_zigzag_table()
+{
+    ZigzagTable t{};
+    for (int v = 0; v < 8; v++)
+        for (int u = 0; u < 8; u++)
+            t.cm[zigzag_index(v, u)] = (uint8_t)(u * 8 + v);
+    return t;
+}
+static __device__ __constant__ ZigzagTable c_zigzag_cm = make_zigzag_table();
 
 /* bits of one non-DC coefficient sent after `run` zeros: table code plus
  * sign, or the escape */
