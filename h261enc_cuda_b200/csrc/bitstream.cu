@@ -7,7 +7,7 @@
  * QCIF / CIF order, macroblocks with MBA, MTYPE, MQUANT, MVD, CBP, TCOEFF
  * and EOB, the last byte zero-padded (src/h261_bitstream.c:64-76).
  *
- * Four launches; the macroblock-parallel ones take contiguous ranges of the
+ * Three launches; the macroblock-parallel ones take contiguous ranges of the
  * step's work list, one warp per macroblock, so that every SM takes part
  * whatever the mix of picture sizes, and kernel boundaries order the
  * phases (nothing waits on a flag):
@@ -25,12 +25,13 @@
  *           picture and GOB headers.
  *   pack    every coded macroblock writes its header and shifts its bit
  *           string into place; a macroblock's first and last word can be
- *           shared with its neighbours and are ORed in with atomics.
- *   copy    the picture into the host arena (mapped pinned memory), at
- *           the offset layout drew with one atomic, split over several
- *           CTAs per picture.
+ *           shared with its neighbours and are ORed in with atomics.  Warps
+ *           count the MBs they finish per picture; the CTA whose count
+ *           completes a picture copies it into the host arena (mapped
+ *           pinned memory) at the offset layout drew with one atomic, and
+ *           writes its record.
  *
- * Layout, pack and copy are programmatic dependent launches: each kernel
+ * Layout and pack are programmatic dependent launches: each kernel
  * of the chain lets the next one launch as soon as its own CTAs are
  * running, and the next one's CTAs wait (griddepcontrol.wait) for the
  * whole previous grid and its memory before they read what it wrote, so
@@ -338,9 +339,8 @@ __global__ void __launch_bounds__(VLC_THREADS) codes_kernel(const h261b_session_
 
 /* ---- layout: one CTA per picture, a warp per GOB (12 warps: all of a CIF
  * picture's GOBs at once); it also draws the picture's place in the host
- * arena, so that the copy can be split over several CTAs */
+ * arena, so that whichever CTA finishes the picture can copy it */
 constexpr int LAYOUT_THREADS = 12 * 32;
-constexpr int COPY_SPLIT = 8;
 
 __global__ void __launch_bounds__(LAYOUT_THREADS) layout_kernel(const h261b_session_dev_t *sessions,
                                                                 h261b_step_dev_t *step, int64_t host_cap)
@@ -466,26 +466,86 @@ __global__ void __launch_bounds__(LAYOUT_THREADS) layout_kernel(const h261b_sess
                 off = (int32_t)a;
         }
         S.vlc_total[2] = off;
+        S.vlc_total[3] = 0;   /* MBs the pack kernel has finished */
         /* the rate control learns the picture's size */
         if (S.rc && S.vlc_total[1] == 0)
             rc_update(*S.rc, S.frame_type, (int32_t)((total + 7) >> 3));
     }
 }
 
-/* ---- pack: headers and coefficient strings into the picture */
-__global__ void __launch_bounds__(VLC_THREADS) pack_kernel(const h261b_session_dev_t *sessions,
-                                                           const uint32_t *work, int32_t n_work)
+/* ---- pack: headers and coefficient strings into the picture; the CTA
+ * that finishes a picture's last MB then copies it into the host arena */
+constexpr int PACK_DONE_MAX = 64;   /* pictures a CTA copies together at its end */
+
+/* a finished picture into the host arena by threads t0, t0 + nt, ..., and
+ * its record (bytes, offset, status, QUANT) by thread t0 */
+__device__ __forceinline__ void copy_picture(const h261b_session_dev_t &S, uint8_t *host_arena, int t0, int nt)
 {
+    const int total = S.vlc_total[0];
+    const int64_t words = ((int64_t)(total + 127) / 128) * 4;
+    const int st = (total < 0 || words * 4 > S.bits_cap) ? H261B_BITS_OVERFLOW : S.vlc_total[1];
+    const int off = st == 0 ? S.vlc_total[2] : -1;
+    const int bytes = (total + 7) >> 3;
+    const int units = ((bytes + 15) & ~15) / 16;
+    if (t0 == 0)
+        *S.pic_out = h261b_pic_info_t{ st == 0 ? bytes : 0, off, st, S.rc ? S.rc->picture_quant : S.quant };
+    if (off < 0 || !host_arena)
+        return;
+    /* other SMs wrote the words: read them from L2 */
+    const uint4 *s4 = reinterpret_cast<const uint4 *>(S.bits_out);
+    uint4 *d4 = reinterpret_cast<uint4 *>(host_arena + off);
+    for (int i = t0; i < units; i += nt)
+        d4[i] = __ldcg(s4 + i);
+}
+
+__global__ void __launch_bounds__(VLC_THREADS) pack_kernel(const h261b_session_dev_t *sessions,
+                                                           const uint32_t *work, int32_t n_work,
+                                                           uint8_t *host_arena)
+{
+    __shared__ int done[PACK_DONE_MAX];
+    __shared__ int n_done;
     pdl_launch_dependents();
     const int lane = threadIdx.x & 31;
+    if (threadIdx.x == 0)
+        n_done = 0;
+    __syncthreads();
     int lo, hi;
     warp_range(n_work, lo, hi);
     pdl_wait();   /* the layout kernel's positions */
+    int run_s = -1, run_n = 0;
+    /* the warp's finished MBs of picture run_s: published once the warp
+     * moves on; the publication that completes the picture queues its copy */
+    auto publish = [&]() {
+        if (run_n == 0)
+            return;
+        const h261b_session_dev_t &P = sessions[run_s];
+        __threadfence();   /* this lane's words before the count */
+        __syncwarp();
+        int k = -1;
+        if (lane == 0 && atomicAdd(&P.vlc_total[3], run_n) + run_n == P.mbw * P.mbh) {
+            k = atomicAdd(&n_done, 1);
+            if (k < PACK_DONE_MAX)
+                done[k] = run_s;
+        }
+        k = __shfl_sync(FULL, k, 0);
+        if (k >= PACK_DONE_MAX) {
+            /* the CTA's list is full: this warp copies the picture now */
+            __threadfence();
+            copy_picture(P, host_arena, lane, 32);
+        }
+        run_n = 0;
+    };
     for (int w = lo; w < hi; w++) {
         const uint32_t item = work[w];
-        const h261b_session_dev_t &S = sessions[item >> 12];
+        const int sidx = (int)(item >> 12);
+        const h261b_session_dev_t &S = sessions[sidx];
         if (!S.bits_out)
             continue;
+        if (sidx != run_s) {
+            publish();
+            run_s = sidx;
+        }
+        run_n++;
         const int mb = (int)(item & 4095u);
         const h261b_mb_info_t r = S.info_out[mb];
         if (r.flags == 0)
@@ -564,31 +624,13 @@ __global__ void __launch_bounds__(VLC_THREADS) pack_kernel(const h261b_session_d
         if (__any_sync(FULL, oob) && lane == 0)
             atomicExch(&S.vlc_total[1], H261B_BITS_MISMATCH);
     }
-}
-
-/* ---- copy: each picture into the host arena, COPY_SPLIT CTAs per picture */
-__global__ void __launch_bounds__(VLC_THREADS) copy_kernel(const h261b_session_dev_t *sessions, uint8_t *host_arena)
-{
-    const h261b_session_dev_t &S = sessions[blockIdx.x];
-    if (!S.bits_out)
-        return;
-    pdl_wait();   /* the packed picture */
-    const int total = S.vlc_total[0];
-    const int64_t words = ((int64_t)(total + 127) / 128) * 4;
-    const int st = (total < 0 || words * 4 > S.bits_cap) ? H261B_BITS_OVERFLOW : S.vlc_total[1];
-    const int off = st == 0 ? S.vlc_total[2] : -1;
-    const int bytes = (total + 7) >> 3;
-    const int units = ((bytes + 15) & ~15) / 16;
-    if (blockIdx.y == 0 && threadIdx.x == 0)
-        *S.pic_out = h261b_pic_info_t{ st == 0 ? bytes : 0, off, st, S.rc ? S.rc->picture_quant : S.quant };
-    if (off < 0 || !host_arena)
-        return;
-    const int per = (units + COPY_SPLIT - 1) / COPY_SPLIT;
-    const int lo = blockIdx.y * per, hi = min(units, lo + per);
-    const uint4 *s4 = reinterpret_cast<const uint4 *>(S.bits_out);
-    uint4 *d4 = reinterpret_cast<uint4 *>(host_arena + off);
-    for (int i = lo + (int)threadIdx.x; i < hi; i += VLC_THREADS)
-        d4[i] = s4[i];
+    publish();
+    __syncthreads();
+    const int nd = min(n_done, PACK_DONE_MAX);
+    for (int i = 0; i < nd; i++) {
+        __threadfence();   /* the other CTAs' words, published before their counts */
+        copy_picture(sessions[done[i]], host_arena, (int)threadIdx.x, VLC_THREADS);
+    }
 }
 
 } // namespace
@@ -694,11 +736,7 @@ extern "C" int h261b_launch_bitstream(h261b_session_dev_t *sessions_dev, int32_t
             return (int)err;
     }
     err = launch_dependent(pack_kernel, dim3(ctas), dim3(VLC_THREADS), st, (const h261b_session_dev_t *)sessions_dev,
-                           work_dev, n_work);
-    if (err != cudaSuccess)
-        return (int)err;
-    err = launch_dependent(copy_kernel, dim3(n_sessions, COPY_SPLIT), dim3(VLC_THREADS), st,
-                           (const h261b_session_dev_t *)sessions_dev, host_arena_dev);
+                           work_dev, n_work, host_arena_dev);
     if (err != cudaSuccess)
         return (int)err;
     return (int)cudaGetLastError();
