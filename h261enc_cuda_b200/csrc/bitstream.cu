@@ -31,11 +31,13 @@
  *           pinned memory) at the offset layout drew with one atomic, and
  *           writes its record.
  *
- * Layout and pack are programmatic dependent launches: each kernel
- * of the chain lets the next one launch as soon as its own CTAs are
- * running, and the next one's CTAs wait (griddepcontrol.wait) for the
- * whole previous grid and its memory before they read what it wrote, so
- * a launch's latency overlaps the kernel before it.
+ * All three are programmatic dependent launches: the kernel before each
+ * one (the encode kernel, codes, layout) lets it launch as soon as its own
+ * CTAs are running, and its CTAs wait (griddepcontrol.wait) for the whole
+ * previous grid and its memory before they read what it wrote, so each
+ * launch's latency overlaps the kernel before it.  The events that mark the
+ * encode kernel's end are recorded on a side stream, so that nothing sits
+ * between the encode kernel and codes in the stream.
  */
 #include <cuda_runtime.h>
 #include <stddef.h>
@@ -215,6 +217,7 @@ __global__ void __launch_bounds__(VLC_THREADS) codes_kernel(const h261b_session_
     uint32_t *stage = sm.stage[warp];
     for (int i = lane; i < MB_WORDS; i += 32)
         stage[i] = 0u;
+    pdl_wait();   /* the encode kernel's records and levels */
     __syncthreads();
 
     const int slot = lane >> 3, j = lane & 7;
@@ -718,7 +721,10 @@ extern "C" int h261b_launch_bitstream(h261b_session_dev_t *sessions_dev, int32_t
     const int codes_ctas = (int)std::min<int64_t>(want, (int64_t)sm_count * codes_res);
     const int ctas = (int)std::min<int64_t>(want, (int64_t)sm_count * pack_res);
     cudaStream_t st = (cudaStream_t)stream;
-    codes_kernel<<<codes_ctas, VLC_THREADS, 0, st>>>(sessions_dev, work_dev, n_work);
+    err = launch_dependent(codes_kernel, dim3(codes_ctas), dim3(VLC_THREADS), st,
+                           (const h261b_session_dev_t *)sessions_dev, work_dev, n_work);
+    if (err != cudaSuccess)
+        return (int)err;
     err = launch_dependent(layout_kernel, dim3(n_sessions), dim3(LAYOUT_THREADS), st,
                                        (const h261b_session_dev_t *)sessions_dev, step,
                                        (int64_t)(host_arena_dev ? host_cap : 0));

@@ -237,6 +237,11 @@ struct h261b_engine_s {
     h261b_engine_config_t cfg;
     int sm_count = 0;
     cudaStream_t stream[2] = { nullptr, nullptr };
+    /* per parity: a side stream that records the events marking the encode
+     * kernel's end, so that nothing sits between the encode kernel and the
+     * bitstream kernel that depends on it (a programmatic dependent launch) */
+    cudaStream_t side[2] = { nullptr, nullptr };
+    cudaEvent_t fork_ev[2] = { nullptr, nullptr }, join_ev[2] = { nullptr, nullptr };
     DevicePool pool;
     std::vector<Session> sessions;
     int32_t open_count = 0;
@@ -407,6 +412,9 @@ extern "C" int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engin
     bool ok = cudaGetDeviceProperties(&prop, cfg->device) == cudaSuccess && h261b_set_quant_table() == 0;
     for (int p = 0; p < 2 && ok; p++) {
         ok = cudaStreamCreateWithFlags(&e->stream[p], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaStreamCreateWithFlags(&e->side[p], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&e->fork_ev[p], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&e->join_ev[p], cudaEventDisableTiming) == cudaSuccess &&
              cudaEventCreateWithFlags(&e->h2d_done[p], cudaEventDisableTiming) == cudaSuccess &&
              cudaEventCreateWithFlags(&e->kernel_done[p], cudaEventDisableTiming) == cudaSuccess &&
              cudaEventCreateWithFlags(&e->step_done[p], cudaEventDisableTiming) == cudaSuccess &&
@@ -480,6 +488,10 @@ extern "C" int h261b_engine_destroy(h261b_engine_t *e)
         cudaEventDestroy(e->t_end[p]);
         if (e->stream[p])
             cudaStreamDestroy(e->stream[p]);
+        if (e->side[p])
+            cudaStreamDestroy(e->side[p]);
+        cudaEventDestroy(e->fork_ev[p]);
+        cudaEventDestroy(e->join_ev[p]);
     }
     if (e->sched_dev)
         cudaFree(e->sched_dev);
@@ -1050,9 +1062,13 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
             set_error("step launch failed: %s", cudaGetErrorString((cudaError_t)lr));
             return H261B_ERR_CUDA;
         }
-        H261B_CUDA_TRY(cudaEventRecordWithFlags(e->k_end[p], st, rf));
-        /* the next step may start encoding while this one writes bitstreams */
-        H261B_CUDA_TRY(cudaEventRecordWithFlags(e->kernel_done[p], st, rf));
+        /* the encode kernel's end, marked on the side stream: the next step
+         * may start encoding while this one writes bitstreams */
+        H261B_CUDA_TRY(cudaEventRecord(e->fork_ev[p], st));
+        H261B_CUDA_TRY(cudaStreamWaitEvent(e->side[p], e->fork_ev[p], 0));
+        H261B_CUDA_TRY(cudaEventRecordWithFlags(e->k_end[p], e->side[p], rf));
+        H261B_CUDA_TRY(cudaEventRecordWithFlags(e->kernel_done[p], e->side[p], rf));
+        H261B_CUDA_TRY(cudaEventRecord(e->join_ev[p], e->side[p]));
         if (n_bits) {
             lr = h261b_launch_bitstream(desc_dev, (int32_t)n, work_dev, n_work, (h261b_step_dev_t *)dm.dev,
                                         e->bits[p].dev, (int64_t)e->bits[p].cap, e->sm_count, st,
@@ -1064,6 +1080,7 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
             H261B_CUDA_TRY(cudaEventRecordWithFlags(e->b_end[p], st, rf));
         }
         H261B_CUDA_TRY(cudaMemcpyAsync(rm.host, rm.dev, d2h, cudaMemcpyDeviceToHost, st));
+        H261B_CUDA_TRY(cudaStreamWaitEvent(st, e->join_ev[p], 0));
         H261B_CUDA_TRY(cudaEventRecordWithFlags(e->t_end[p], st, rf));
         H261B_CUDA_TRY(cudaEventRecordWithFlags(e->step_done[p], st, rf));
         return H261B_OK;

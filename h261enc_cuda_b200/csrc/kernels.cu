@@ -844,6 +844,9 @@ __global__ void __launch_bounds__(256, H261B_STEP_MIN_BLOCKS)
                 int32_t chunk, int32_t phases, int32_t *sched)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    /* the bitstream kernel after this one may launch now; it waits for the
+     * whole grid before it reads anything (griddepcontrol.wait) */
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     WarpSmem &sm = reinterpret_cast<WarpSmem *>(smem_raw)[warp];
     const int warps = blockDim.x >> 5;
