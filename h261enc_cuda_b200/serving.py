@@ -12,7 +12,8 @@ is admitted.  The loop:
   release time has come (continuous batching: a session admitted while
   others are on the GPU joins the next step), copies them on the engine's
   threads while the previous step is read, and issues one step;
-* reads each step's bitstreams one step later and records, per picture, the
+* reads each step's bitstreams one step later (a picture that did not fit
+  the host arena is read from the device) and records, per picture, the
   latency from its release to its bitstream on the host;
 * closes a session once its last picture has been read.
 
@@ -162,10 +163,18 @@ class Server:
             now = clock() - t0
             for sid, release in in_step.pop(k):
                 s, p = live[sid], got[sid]
-                if p["status"] != 0:
+                if p["status"] == 1:
+                    # the picture did not fit the host arena (the engine
+                    # grows it for later steps): read it from the device
+                    bits = e.result(sid, copy=False).bits
+                    if bits is None:
+                        raise RuntimeError(f"session {s.req.rid}: picture {s.done} has no bitstream")
+                elif p["status"] != 0:
                     raise RuntimeError(f"session {s.req.rid}: picture {s.done} has no bitstream")
+                else:
+                    bits = None
                 if s.bits is not None:
-                    s.bits.append(ctypes.string_at(int(p["bits"]), int(p["bytes"])))
+                    s.bits.append(bits if bits is not None else ctypes.string_at(int(p["bits"]), int(p["bytes"])))
                 s.done += 1
                 if now <= duration or drain:
                     lat.append((now - release) * 1e3)

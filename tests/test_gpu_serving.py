@@ -34,3 +34,20 @@ def test_served_sessions_equal_their_alone_encodes(gpu):
         assert b"".join(got) == want, f"request {r.rid}"
     summ = st.summary()
     assert summ["latency_ms"]["p50"] is not None and summ["latency_ms"]["p99"] >= summ["latency_ms"]["p50"]
+
+
+def test_served_sessions_survive_a_full_host_arena(gpu):
+    """With a host bitstream arena far too small for a step, pictures that do
+    not fit are read from the device, and every stream is still its alone
+    encode."""
+    reqs = serving.poisson_requests(40, 1.0, seed=12, frames=(3, 8))
+    keep = [r.rid for r in reqs]
+    pool = serving.ClipPool(clips_per_size=2, length=8)
+    with Engine(max_sessions=64, levels_to_host=0, bits_host_bytes=4096, warps_per_cta=4) as e:
+        srv = serving.Server(e, pool, fps=30.0, keep_bits_for=keep)
+        st = srv.run(reqs, duration=1.0, drain=True)
+    assert st.pictures == sum(r.frames for r in reqs)
+    for r in reqs:
+        frames = np.stack([pool.frame(r.width, r.height, r.seed, i) for i in range(r.frames)])
+        want = O.encode_stream(frames, r.width, r.height, quant=r.quant)[0]
+        assert b"".join(srv.bits[r.rid]) == want, f"request {r.rid}"
