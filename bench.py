@@ -342,9 +342,10 @@ def ours(args, world, rank, local, dist):
     # in HBM (the bitstream is the output)
     eng = Engine(device=local, max_sessions=4 * len(streams), levels_to_host=0)
     run = Runner(eng, streams, pools)
-    # warm-up (includes the launch-shape tuning steps), both input paths
+    # warm-up (includes the launch-shape tuning steps), both input paths on
+    # both step parities
     for i in range(max(args.warmup, 8)):
-        run.queue_device() if i % 2 else run.queue_host()
+        run.queue_device() if (i // 2) % 2 else run.queue_host()
         eng.step()
         eng.sync()
         run.retire(run.queued - 1)
@@ -478,7 +479,7 @@ def ours(args, world, rank, local, dist):
         # the committed ncu figure is for batch64
         "issue_roofline": (issue_roofline(mb_per_step, mean_kernel, local, clk.summary())
                            if args.workload == "batch64" else None),
-        "gpu_launches": 5 * args.steps,   # encode + codes, layout, pack, copy
+        "gpu_launches": 4 * args.steps,   # encode, codes, layout, pack (which also copies)
         "graphs": {"captures": graph_caps, "replays": graph_reps,
                    "note": "steps whose launch signature repeats replay a captured CUDA graph"},
         "clocks": clk.summary(),
@@ -506,8 +507,15 @@ def serve(args, world, rank, local, dist):
     torch.cuda.set_device(local)
     reqs = serving.poisson_requests(200.0, args.serve_seconds, seed=100 + rank)
     pool = serving.ClipPool()
-    with Engine(device=local, max_sessions=8192, levels_to_host=0, hbm_budget_bytes=40 << 30) as e:
+    # the host bitstream arena holds the largest step the run can pile up
+    with Engine(device=local, max_sessions=8192, levels_to_host=0, hbm_budget_bytes=40 << 30,
+                bits_host_bytes=256 << 20) as e:
         srv = serving.Server(e, pool, fps=30.0)
+        # capacity plan before the first arrival: the sessions open at once
+        # in steady state at this rate and mean length (Little's law)
+        mean_frames = (30 + 600) / 2
+        srv.plan({(176, 144): serving.expected_concurrency(200.0, mean_frames, 30.0, 0.7),
+                  (352, 288): serving.expected_concurrency(200.0, mean_frames, 30.0, 0.3)})
         if dist:
             dist.barrier()
         with ClockSampler(local) as clk:
@@ -522,7 +530,7 @@ def serve(args, world, rank, local, dist):
                 "config": {"workload": "serve", "seconds": args.serve_seconds, "arrival_rate": 200,
                            "sessions": len(reqs), "hbm_budget_gb": 40},
                 "latency_ms": summ["latency_ms"], "latency_ms_second_half": summ["latency_ms_second_half"],
-                "serving": summ, "gpu_launches": 5 * st.steps,
+                "serving": summ, "gpu_launches": 4 * st.steps,
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     if dist:

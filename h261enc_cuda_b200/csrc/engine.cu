@@ -82,6 +82,26 @@ class DevicePool {
         return H261B_OK;
     }
     void put(size_t bytes, void *p) { free_[align_up(bytes, 256)].push_back(p); }
+    /* at least `count` free blocks of this size, in slabs of up to 1 GiB */
+    int reserve(size_t bytes, size_t count)
+    {
+        bytes = align_up(bytes, 256);
+        auto &fl = free_[bytes];
+        while (fl.size() < count) {
+            const size_t per = std::max<size_t>(1, std::min<size_t>(count - fl.size(), (size_t)(1u << 30) / bytes));
+            void *slab = nullptr;
+            cudaError_t err = cudaMalloc(&slab, per * bytes);
+            if (err != cudaSuccess) {
+                set_error("device pool: cudaMalloc(%zu) failed: %s", per * bytes, cudaGetErrorString(err));
+                return H261B_ERR_NOMEM;
+            }
+            slabs_.push_back(slab);
+            held_ += per * bytes;
+            for (size_t i = 0; i < per; i++)
+                fl.push_back((char *)slab + i * bytes);
+        }
+        return H261B_OK;
+    }
     int64_t held() const { return (int64_t)held_; }
 
   private:
@@ -102,7 +122,7 @@ struct Mirror {
             return H261B_OK;
         /* doubling: a growing session count reallocates (and syncs) only a
          * few times */
-        size_t c = align_up(std::max<size_t>(std::max<size_t>(bytes, 1 << 16), 2 * cap), 4096);
+        size_t c = align_up(std::max<size_t>(std::max<size_t>(bytes, 1 << 20), 2 * cap), 4096);
         uint8_t *nh = nullptr, *nd = nullptr;
         cudaError_t e1 = cudaMallocHost(&nh, c);
         cudaError_t e2 = cudaMalloc(&nd, c);
@@ -145,6 +165,12 @@ struct StepKey {
 struct StepGraph {
     cudaGraphExec_t exec = nullptr;
     StepKey key;
+    /* the signature of the last step launched directly on this parity: a
+     * graph is captured only for a signature seen twice in a row, so that
+     * steps whose sessions keep changing (one stream at a time, serving)
+     * do not pay a capture each */
+    StepKey last_direct;
+    bool has_last_direct = false;
     void reset()
     {
         if (exec)
@@ -245,8 +271,6 @@ struct h261b_engine_s {
     DevicePool pool;
     std::vector<Session> sessions;
     int32_t open_count = 0;
-    size_t sum_upload = 0, sum_results = 0;   /* arena shares of the open sessions */
-    int64_t sum_mb = 0;
     int64_t session_bytes = 0;
 
     Mirror upload[2];          /* queued source pictures                  */
@@ -266,6 +290,8 @@ struct h261b_engine_s {
      * start (the previous step's encode is done), results downloaded */
     cudaEvent_t t_begin[2] = { nullptr, nullptr }, t_h2d[2] = { nullptr, nullptr };
     cudaEvent_t t_ready[2] = { nullptr, nullptr }, t_end[2] = { nullptr, nullptr };
+    /* step arena bytes asked for by h261b_engine_reserve_step */
+    size_t reserved_upload = 0, reserved_results = 0, reserved_desc = 0;
     /* the encode launches' work counters, two per stream (h261b_launch_step) */
     int32_t *sched_dev = nullptr;
     bool step_bits_ran[2] = { false, false };
@@ -432,6 +458,15 @@ extern "C" int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engin
         return H261B_ERR_CUDA;
     }
     e->sm_count = prop.multiProcessorCount;
+    if (cfg->bits_host_bytes > 0) {
+        /* a configured host bitstream arena is allocated now, not by the
+         * first steps */
+        for (int p = 0; p < 2; p++)
+            if (e->bits[p].reserve(e->bits_want) != H261B_OK) {
+                h261b_engine_destroy(e);
+                return H261B_ERR_NOMEM;
+            }
+    }
     bool cached = false;
     if (cfg->warps_per_cta == 0) {
         std::lock_guard<std::mutex> lk(g_tuned_mu);
@@ -506,14 +541,6 @@ static Session *get_session(h261b_engine_t *e, int32_t id)
         return nullptr;
     }
     return &e->sessions[(size_t)id];
-}
-
-/* arena bytes a step takes at most for one session (every open session
- * may have a picture in it); kept as running sums over the open sessions */
-static size_t upload_share(const Session &s) { return align_up(s.lay.bytes, 256); }
-static size_t results_share(const Session &s)
-{
-    return (size_t)s.nmb * sizeof(h261b_mb_info_t) + sizeof(h261b_pic_info_t) + 32 + align_up((size_t)s.nmb * 384, 256);
 }
 
 extern "C" int h261b_session_open(h261b_engine_t *e, const h261b_session_config_t *c, int32_t *id)
@@ -612,11 +639,49 @@ extern "C" int h261b_session_open(h261b_engine_t *e, const h261b_session_config_
     H261B_CUDA_TRY(cudaMemcpyAsync(s.dn, &dn0, sizeof(dn0), cudaMemcpyHostToDevice, st));
     s.open = true;
     e->open_count++;
-    e->sum_upload += upload_share(s);
-    e->sum_results += results_share(s);
-    e->sum_mb += s.nmb;
     e->session_bytes += need;
     *id = slot;
+    return H261B_OK;
+}
+
+extern "C" int h261b_engine_reserve(h261b_engine_t *e, const h261b_session_config_t *c, int32_t count)
+{
+    clear_error();
+    if (!e || count < 0 || !session_config_ok(c)) {
+        set_error("h261b_engine_reserve: bad arguments");
+        return H261B_ERR_ARG;
+    }
+    const int64_t need = h261b_session_config_bytes(c);
+    if (need <= 0) {
+        set_error("h261b_engine_reserve: bad session configuration");
+        return H261B_ERR_ARG;
+    }
+    cudaSetDevice(e->cfg.device);
+    return e->pool.reserve((size_t)need, (size_t)count);
+}
+
+static int grow_arenas(h261b_engine_t *e, int p, size_t up, size_t keep, size_t res, size_t desc);
+
+extern "C" int h261b_engine_reserve_step(h261b_engine_t *e, const h261b_session_config_t *c, int32_t pictures)
+{
+    clear_error();
+    if (!e || pictures < 0 || !session_config_ok(c)) {
+        set_error("h261b_engine_reserve_step: bad arguments");
+        return H261B_ERR_ARG;
+    }
+    cudaSetDevice(e->cfg.device);
+    const PictureLayout lay = PictureLayout::of(c->width, c->height);
+    const size_t nmb = (size_t)(c->width / 16) * (c->height / 16), k = (size_t)pictures;
+    e->reserved_upload += k * align_up(lay.bytes, 256);
+    e->reserved_results += k * (nmb * sizeof(h261b_mb_info_t) + sizeof(h261b_pic_info_t) + 32 +
+                                align_up(nmb * 384, 256)) + 1024;
+    e->reserved_desc += k * (sizeof(h261b_session_dev_t) + nmb * sizeof(uint32_t)) + 1024;
+    for (int p = 0; p < 2; p++) {
+        const size_t keep = (p == (int)(e->next_step & 1) && e->upload_checked) ? e->upload_used : 0;
+        int rc = grow_arenas(e, p, e->reserved_upload, keep, e->reserved_results, e->reserved_desc);
+        if (rc)
+            return rc;
+    }
     return H261B_OK;
 }
 
@@ -632,31 +697,26 @@ extern "C" int h261b_session_close(h261b_engine_t *e, int32_t id)
     reclaim(e);
     e->session_bytes -= (int64_t)s->slot_bytes;
     e->open_count--;
-    e->sum_upload -= upload_share(*s);
-    e->sum_results -= results_share(*s);
-    e->sum_mb -= s->nmb;
     *s = Session();
     return H261B_OK;
 }
 
-/* grow the arenas of parity p to hold a step of every open session; the
- * queued part of the upload arena is kept, arenas of the other parity (the
- * previous step, still readable by the caller) are not touched */
-static int ensure_capacity(h261b_engine_t *e, int p)
+/* Grow the arenas of parity p to hold `up` upload bytes (the first `keep`
+ * of which are queued pictures that survive), `res` result bytes and `desc`
+ * descriptor bytes.  Sized by what a step actually holds, not by every open
+ * session, so that a server with thousands of open sessions and a few
+ * pictures per step keeps small arenas; they grow by doubling, so a
+ * growing load reallocates (and waits for the parity's stream) a few times
+ * only. */
+static int grow_arenas(h261b_engine_t *e, int p, size_t up, size_t keep, size_t res, size_t desc)
 {
-    const size_t up = e->sum_upload;
-    const size_t res = e->sum_results + 512;   /* alignment of the record, picture and level regions */
-    const size_t desc = sizeof(h261b_step_dev_t) + align_up((size_t)e->open_count * sizeof(h261b_session_dev_t), 256) +
-                        (size_t)e->sum_mb * sizeof(uint32_t);
-    if (up > e->upload[p].cap || res > e->results[p].cap || desc > e->desc[p].cap) {
-        e->copier->join();   /* copies in flight write into the upload arena */
-        H261B_CUDA_TRY(cudaStreamSynchronize(e->stream[p]));
-        int rc;
-        const size_t keep = e->upload_checked ? e->upload_used : 0;
-        if ((rc = e->upload[p].reserve(up, keep)) || (rc = e->results[p].reserve(res)) ||
-            (rc = e->desc[p].reserve(desc)))
-            return rc;
-    }
+    if (up <= e->upload[p].cap && res <= e->results[p].cap && desc <= e->desc[p].cap)
+        return H261B_OK;
+    e->copier->join();   /* copies in flight write into the upload arena */
+    H261B_CUDA_TRY(cudaStreamSynchronize(e->stream[p]));
+    int rc;
+    if ((rc = e->upload[p].reserve(up, keep)) || (rc = e->results[p].reserve(res)) || (rc = e->desc[p].reserve(desc)))
+        return rc;
     return H261B_OK;
 }
 
@@ -672,9 +732,6 @@ static int reserve_input(h261b_engine_t *e, Session *s, int32_t id, int32_t quan
         return H261B_ERR_STATE;
     }
     const int p = (int)(e->next_step & 1);
-    int rc = ensure_capacity(e, p);
-    if (rc)
-        return rc;
     if (!e->upload_checked) {
         /* the copy that last read this pinned arena (two steps ago) must be
          * complete before the host writes into it */
@@ -684,6 +741,9 @@ static int reserve_input(h261b_engine_t *e, Session *s, int32_t id, int32_t quan
         e->upload_used = 0;
     }
     *off = e->upload_used;
+    int rc = grow_arenas(e, p, *off + align_up(s->lay.bytes, 256), e->upload_used, 0, 0);
+    if (rc)
+        return rc;
     if (*off + s->lay.bytes > e->upload[p].cap) {
         set_error("%s: upload arena overflow", who);
         return H261B_ERR_STATE;
@@ -730,6 +790,22 @@ extern "C" int h261b_engine_inputs(h261b_engine_t *e, int32_t n, const int32_t *
             set_error("h261b_engine_inputs: session %d is not open", ids[i]);
             return H261B_ERR_ARG;
         }
+    /* room for the whole batch at once: one reallocation at most */
+    {
+        const int p = (int)(e->next_step & 1);
+        if (!e->upload_checked) {
+            if (e->in_flight[p])
+                H261B_CUDA_TRY(cudaEventSynchronize(e->h2d_done[p]));
+            e->upload_checked = true;
+            e->upload_used = 0;
+        }
+        size_t need = e->upload_used;
+        for (int32_t i = 0; i < n; i++)
+            need += align_up(e->sessions[(size_t)ids[i]].lay.bytes, 256);
+        int rc = grow_arenas(e, p, need, e->upload_used, 0, 0);
+        if (rc)
+            return rc;
+    }
     const size_t used0 = e->upload_used;
     for (int32_t i = 0; i < n; i++) {
         Session *s = get_session(e, ids[i]);
@@ -895,9 +971,28 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
             list.push_back((int32_t)i);
     if (list.empty())
         return 0;
-    int rc = ensure_capacity(e, p);
-    if (rc)
-        return rc;
+    /* this step's descriptor and result bytes (the layouts below) */
+    {
+        int64_t mbs = 0;
+        size_t levels = 0;
+        for (int32_t sid : list) {
+            mbs += e->sessions[(size_t)sid].nmb;
+            levels += align_up((size_t)e->sessions[(size_t)sid].nmb * 384, 256);
+        }
+        const size_t n_list = list.size();
+        const size_t res = align_up(align_up(align_up((size_t)mbs * sizeof(h261b_mb_info_t), 256) +
+                                                 n_list * sizeof(h261b_pic_info_t),
+                                             256) +
+                                        n_list * 32,
+                                    256) +
+                           levels;
+        const size_t desc = sizeof(h261b_step_dev_t) + align_up(n_list * sizeof(h261b_session_dev_t), 256) +
+                            (size_t)mbs * sizeof(uint32_t);
+        int rc = grow_arenas(e, p, 0, 0, res, desc);
+        if (rc)
+            return rc;
+    }
+    int rc;
     /* arenas of this parity were last used by step id-2 */
     if (e->in_flight[p] && id - 2 > e->done_step) {
         H261B_CUDA_TRY(cudaEventSynchronize(e->step_done[p]));
@@ -1089,15 +1184,23 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
     /* Steps whose launches look the same (sizes, arena addresses, launch
      * shape) replay one CUDA graph per parity: the descriptor and work-list
      * contents differ, but they are data in pinned memory that the graph's
-     * upload copies.  Tuning steps, an engine's first step and engines with
-     * use_graphs = 0 launch directly. */
+     * upload copies.  A signature is captured the second time in a row it
+     * comes on its parity.  Tuning steps, an engine's first step and engines
+     * with use_graphs = 0 launch directly. */
     const StepKey key = { dm.host, dm.dev, um.host, um.dev, rm.host, rm.dev, bits_dev_or_null(e, p, n_bits),
                           n_bits ? e->bits[p].cap : 0, desc_off, work_off, desc_bytes, upload_bytes, ssd_base,
                           d2h, (int64_t)n, n_work, rc_begin, n_rc, n_ssd ? 1 : 0, warps, ctas, phases,
                           id > 0 ? 1 : 0 };
     StepGraph &gr = e->graph[p];
+    const bool repeated = gr.has_last_direct && gr.last_direct == key;
     const bool capturable = e->cfg.use_graphs && !e->graphs_off && !tuning && id > 0;
-    if (capturable && gr.exec && gr.key == key) {
+    if (capturable && !(gr.exec && gr.key == key) && !repeated) {
+        /* a new signature: launch directly, capture if it comes again */
+        gr.last_direct = key;
+        gr.has_last_direct = true;
+        if ((rc = enqueue(false)))
+            return rc;
+    } else if (capturable && gr.exec && gr.key == key) {
         H261B_CUDA_TRY(cudaGraphLaunch(gr.exec, st));
         e->graph_replays++;
     } else if (capturable && cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {

@@ -80,6 +80,19 @@ class Engine:
         self._dims[sid.value] = (width, height)
         return sid.value
 
+    def reserve(self, width: int, height: int, count: int, bitstream: int = 0, rate_control: int = 0,
+                bitrate: int = 0) -> None:
+        """Allocate the device blocks of ``count`` sessions of this shape now,
+        so that opening them later allocates nothing."""
+        c = _lib.SessionConfig(width, height, 8, 0, 5, bitstream, rate_control, bitrate, 0)
+        check(_lib.core().h261b_engine_reserve(self._h, ctypes.byref(c), count), "h261b_engine_reserve")
+
+    def reserve_step(self, width: int, height: int, pictures: int) -> None:
+        """Size the step arenas for ``pictures`` more pictures of this size
+        in one step, so that steps up to that size never reallocate them."""
+        c = _lib.SessionConfig(width, height, 8, 0, 5, 0, 0, 0, 0)
+        check(_lib.core().h261b_engine_reserve_step(self._h, ctypes.byref(c), pictures), "h261b_engine_reserve_step")
+
     def close(self, sid: int) -> None:
         check(_lib.core().h261b_session_close(self._h, sid), "h261b_session_close")
         self._dims.pop(sid, None)

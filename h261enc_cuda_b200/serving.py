@@ -25,7 +25,9 @@ what the session produces alone (tests/test_gpu_serving.py checks it).
 from __future__ import annotations
 
 import ctypes
+import gc
 import heapq
+import math
 import time
 from collections import deque
 from dataclasses import dataclass, field
@@ -121,6 +123,13 @@ class ServeStats:
         }
 
 
+def expected_concurrency(rate: float, mean_frames: float, fps: float, share: float, margin: float = 1.25) -> int:
+    """Sessions of one kind open at once in steady state (Little's law:
+    arrival rate x time in the system), with a margin: the capacity a server
+    plans for a Poisson stream of known rate and length distribution."""
+    return int(math.ceil(rate * share * mean_frames / fps * margin))
+
+
 class Server:
     """The request loop around one engine (which must have been created
     with the HBM budget that admission obeys)."""
@@ -132,11 +141,36 @@ class Server:
         self.keep = set(keep_bits_for)      # request ids whose bitstreams are kept (tests)
         self.bits: Dict[int, List[bytes]] = {}
 
+    def plan(self, capacity: Dict[tuple, int], burst: float = 0.5) -> None:
+        """Allocate the device blocks of {(width, height): sessions} up front,
+        so that admissions during the run take pooled blocks, and size the
+        step arenas for a step holding `burst` of those sessions' pictures
+        (what piles up if the loop falls behind by burst / fps seconds)."""
+        for (w, h), n in capacity.items():
+            self.e.reserve(w, h, n, bitstream=1)
+            self.e.reserve_step(w, h, int(math.ceil(n * burst)))
+
     def run(self, requests: List[Request], duration: float, drain: bool = False,
             clock=time.perf_counter) -> ServeStats:
         """Serve `requests` (arrival times within `duration` seconds).  The
         statistics cover [0, duration]; with drain=True the sessions still
-        running then are encoded to their end first, else they are closed."""
+        running then are encoded to their end first, else they are closed.
+
+        Python's cyclic garbage collector is off while the loop runs: its
+        full passes paused the loop for 40-70 ms, long enough for a step's
+        worth of pictures from every session to pile up behind it.  The
+        loop's objects hold no reference cycles, so reference counting
+        frees them all."""
+        enabled = gc.isenabled()
+        gc.collect()
+        gc.disable()
+        try:
+            return self._run(requests, duration, drain, clock)
+        finally:
+            if enabled:
+                gc.enable()
+
+    def _run(self, requests, duration, drain, clock) -> ServeStats:
         e, fps = self.e, self.fps
         arrivals = deque(sorted(requests, key=lambda r: r.arrival))
         waiting: deque = deque()

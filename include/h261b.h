@@ -107,6 +107,15 @@ int64_t h261b_session_config_bytes(const h261b_session_config_t *cfg);
 
 int h261b_session_open(h261b_engine_t *e, const h261b_session_config_t *cfg, int32_t *session_id);
 int h261b_session_close(h261b_engine_t *e, int32_t session_id);
+/* Allocate the device blocks of `count` sessions of this configuration
+ * ahead of their opening (capacity planning for a server: opens then take
+ * a block from the pool without allocating).  The blocks count against no
+ * budget until a session holds them. */
+int h261b_engine_reserve(h261b_engine_t *e, const h261b_session_config_t *cfg, int32_t count);
+/* Size both step arenas (upload, results, descriptors) for `pictures`
+ * pictures of this configuration in one step, on top of what earlier calls
+ * reserved: steps up to that size never reallocate an arena. */
+int h261b_engine_reserve_step(h261b_engine_t *e, const h261b_session_config_t *cfg, int32_t pictures);
 
 /* Queue the session's next source picture (packed planes: Y stride W,
  * chroma stride W/2); the bytes are copied before the call returns.

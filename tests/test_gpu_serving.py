@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from h261enc_cuda_b200 import serving
+from h261enc_cuda_b200 import serving, synth
 from h261enc_cuda_b200.engine import Engine, session_config_bytes
 
 pytestmark = pytest.mark.gpu
@@ -51,3 +51,22 @@ def test_served_sessions_survive_a_full_host_arena(gpu):
         frames = np.stack([pool.frame(r.width, r.height, r.seed, i) for i in range(r.frames)])
         want = O.encode_stream(frames, r.width, r.height, quant=r.quant)[0]
         assert b"".join(srv.bits[r.rid]) == want, f"request {r.rid}"
+
+
+def test_reserved_blocks_serve_later_opens(gpu):
+    """Blocks reserved up front are what later sessions get: opening them
+    allocates no more device memory."""
+    with Engine(max_sessions=64, levels_to_host=0, warps_per_cta=4) as e:
+        e.reserve(176, 144, 12, bitstream=1)
+        e.reserve(352, 288, 5, bitstream=1)
+        held = e.stats()[2]
+        assert held >= 12 * session_config_bytes(176, 144, bitstream=1) + 5 * session_config_bytes(352, 288,
+                                                                                                  bitstream=1)
+        sids = [e.open(176, 144, 8, bitstream=1) for _ in range(12)] + \
+               [e.open(352, 288, 8, bitstream=1) for _ in range(5)]
+        assert e.stats()[2] == held
+        fr = synth.clip(0, 176, 144, 3, 1)[0]
+        e.submit_frame(sids[0], fr)
+        e.step()
+        e.sync()
+        assert e.result(sids[0]).bits

@@ -91,3 +91,26 @@ def test_every_picture_once_in_order_and_budget_admission(monkeypatch):
     assert st.latencies_ms.size == st.pictures and (st.latencies_ms >= 0).all()
     if len(reqs) > 4:
         assert st.refused_at_least_once > 0
+
+
+def test_capacity_plan_follows_littles_law():
+    # 200 sessions/s, 315 pictures at 30 per second: 2,100 open at once
+    assert serving.expected_concurrency(200.0, 315.0, 30.0, 1.0, margin=1.0) == 2100
+    qcif = serving.expected_concurrency(200.0, 315.0, 30.0, 0.7)
+    cif = serving.expected_concurrency(200.0, 315.0, 30.0, 0.3)
+    assert qcif + cif >= 2100 * 1.25
+
+    class Recorder:
+        def __init__(self):
+            self.calls = []
+
+        def reserve(self, w, h, n, bitstream=0):
+            self.calls.append(("blocks", w, h, n, bitstream))
+
+        def reserve_step(self, w, h, n):
+            self.calls.append(("step", w, h, n))
+
+    rec = Recorder()
+    serving.Server(rec, None).plan({(176, 144): qcif, (352, 288): cif}, burst=0.5)
+    assert rec.calls == [("blocks", 176, 144, qcif, 1), ("step", 176, 144, -(-qcif // 2)),
+                         ("blocks", 352, 288, cif, 1), ("step", 352, 288, -(-cif // 2))]
