@@ -19,7 +19,11 @@
  * usage: h261_drive in=<yuv> w=<W> h=<H> frames=<N> bits=<out.h261>
  *                   recon=<out.yuv> dump=<out.bin>
  *                   [quant=<1..31> | bitrate=<bit/s>] [intra=<period>]
- *                   [denoise=<d>]
+ *                   [denoise=<d>] [timing=<out.txt>]
+ *
+ * timing= writes the milliseconds each picture took from its upload to its
+ * reconstruction (the boundary calls and the host mode decision, rate
+ * control and writers, not the file reads and dumps), one line per picture.
  *
  * Dump record per frame (little endian):
  *   "H261FRM1", int32 frame, frame_type, picture_quant, num_mb, bytes,
@@ -72,6 +76,8 @@ int main(int argc, char **argv)
     Int32 bitrate = atoi(arg(argc, argv, "bitrate", "384000"));
     Int32 intra_period = atoi(arg(argc, argv, "intra", "0"));
     Int32 denoise = atoi(arg(argc, argv, "denoise", "5"));
+    const char *timing_path = arg(argc, argv, "timing", NULL);
+    FILE *ftime = timing_path ? fopen(timing_path, "w") : NULL;
     if (!in_path || !bits_path || !recon_path || !dump_path ||
         !((w == 176 && h == 144) || (w == 352 && h == 288))) {
         fprintf(stderr, "usage: h261_drive in= w= h= frames= bits= recon= dump= [quant=|bitrate=] [intra=] [denoise=]\n");
@@ -111,6 +117,7 @@ int main(int argc, char **argv)
             status = 4;
             break;
         }
+        const double t0 = h261_get_time();
         h261_gpu_device_set_current(src->pui8_Y, w, h);
         h261_gpu_device_set_current_chroma_cb(src->pui8_Cb, w / 2, h / 2);
         h261_gpu_device_set_current_chroma_cr(src->pui8_Cr, w / 2, h / 2);
@@ -154,6 +161,8 @@ int main(int argc, char **argv)
         memcpy(ref->pui8_Y, mbs->pui8_reconstructed_Y_host, fsize);
         memcpy(ref->pui8_Cb, mbs->pui8_reconstructed_Cb_host, fsize / 4);
         memcpy(ref->pui8_Cr, mbs->pui8_reconstructed_Cr_host, fsize / 4);
+        if (ftime)
+            fprintf(ftime, "%.4f\n", h261_get_time() - t0);
         fwrite(ref->pui8_Y, fsize, 1, frec);
         fwrite(ref->pui8_Cb, fsize / 4, 1, frec);
         fwrite(ref->pui8_Cr, fsize / 4, 1, frec);
@@ -179,5 +188,7 @@ int main(int argc, char **argv)
     fclose(fbits);
     fclose(frec);
     fclose(fdump);
+    if (ftime)
+        fclose(ftime);
     return status;
 }
