@@ -59,6 +59,7 @@ PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "step_kernel_batch64.md")
 ALG_BYTES_PER_MB = 384 + 384 + 384 + 384 + 16 + 4
 # reference-mode search: 121 + 49 candidates x 256 absolute differences
 SAD_PER_MB = 170 * 256
+SAD_PER_MB_FULL = 961 * 256
 
 
 def parse():
@@ -68,6 +69,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=8)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batch64", choices=["batch64", "stress1024", "serve"])
+    ap.add_argument("--me", default="reference", choices=["reference", "full"],
+                    help="motion search: the reference's grid + refinement (bit-exact), or every vector "
+                         "of [-15,15]^2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=20.0,
                     help="length of the serving run (--workload serve)")
@@ -340,7 +344,8 @@ def ours(args, world, rank, local, dist):
 
     # every stream writes its H.261 bitstream on the device; the levels stay
     # in HBM (the bitstream is the output)
-    eng = Engine(device=local, max_sessions=4 * len(streams), levels_to_host=0)
+    me_mode = 1 if args.me == "full" else 0
+    eng = Engine(device=local, max_sessions=4 * len(streams), levels_to_host=0, me_mode=me_mode)
     run = Runner(eng, streams, pools)
     # warm-up (includes the launch-shape tuning steps), both input paths on
     # both step parities
@@ -421,7 +426,7 @@ def ours(args, world, rank, local, dist):
 
     # ---- single stream: the same streams one at a time, one picture per step
     single_lat, single_mbs = [], 0
-    eng1 = Engine(device=local, max_sessions=8, warps_per_cta=4, levels_to_host=0)
+    eng1 = Engine(device=local, max_sessions=8, warps_per_cta=4, levels_to_host=0, me_mode=me_mode)
     per_stream = 3
     t0 = time.perf_counter()
     for k, s in enumerate(streams):
@@ -450,7 +455,7 @@ def ours(args, world, rank, local, dist):
     mean_ms = total_ms / args.steps
     achieved = mb_per_step * ALG_BYTES_PER_MB / (mean_kernel * 1e-3) / 1e9
     tr = ncu_traffic_per_mb()
-    sad_rate = mb_per_step * SAD_PER_MB / (mean_kernel * 1e-3)
+    sad_rate = mb_per_step * (SAD_PER_MB_FULL if me_mode else SAD_PER_MB) / (mean_kernel * 1e-3)
     line = {
         "metric": METRICS[args.workload],
         "value": value, "unit": "MB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -459,7 +464,8 @@ def ours(args, world, rank, local, dist):
                                 "stress1024": "synthetic (per-16x16-block random motion in [-15,15] plus noise, "
                                               "24-picture ping-pong per stream)"}[args.workload],
         "config": {"workload": args.workload, "streams": len(streams), "mb_per_step": mb_per_step,
-                   "me_mode": "reference (11x11 grid + 7x7 refinement)",
+                   "me_mode": ("full (every vector of [-15,15]^2; not bit-exact to the reference)" if me_mode
+                               else "reference (11x11 grid + 7x7 refinement)"),
                    "l2": "flushed before every timed step (256 MiB write)", "parallelism": f"sessions x{world}"},
         "kernels_ms": {"encode": mean_kernel, "bitstream": float(np.mean(bits_ms))},
         "bitstream_bytes_per_step": float(np.mean(bits_bytes)),
@@ -476,9 +482,9 @@ def ours(args, world, rank, local, dist):
                      "traffic": (tr * mb_per_step) if tr else None},
         "sad_roofline": {"achieved": sad_rate, "peak": peak_sad, "unit": "absdiff/s", "frac": sad_rate / peak_sad,
                          "peak_source": "project microbenchmark of the search's SAD step"},
-        # the committed ncu figure is for batch64
+        # the committed ncu figure is for batch64 in reference mode
         "issue_roofline": (issue_roofline(mb_per_step, mean_kernel, local, clk.summary())
-                           if args.workload == "batch64" else None),
+                           if args.workload == "batch64" and not me_mode else None),
         "gpu_launches": 4 * args.steps,   # encode, codes, layout, pack (which also copies)
         "graphs": {"captures": graph_caps, "replays": graph_reps,
                    "note": "steps whose launch signature repeats replay a captured CUDA graph"},
