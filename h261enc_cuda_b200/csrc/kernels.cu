@@ -209,6 +209,69 @@ __device__ __forceinline__ void sad16x16_pair(const StageBuf s, int vx0, int vy0
     s1 = c0 + c1;
 }
 
+/* SADs of the source MB against N window blocks stacked one row apart:
+ * the vectors (vx, vy0 + k), k < N, with vx in [-15, 15] and vy0 in
+ * [-15, 16 - N].  Window row R serves candidate k with source row R - k,
+ * so each of the 15 + N window rows is loaded and aligned once for all N
+ * candidates (the pair above loads and aligns 16 rows per candidate).
+ * Rows R < N - 1 and R > 15 reach only some candidates; they are unrolled
+ * apart from the steady rows in between. */
+template <int N>
+__device__ __forceinline__ void sad16x16_column(const StageBuf s, int vx, int vy0, uint32_t sad[N])
+{
+    const int b = 16 + vx;
+    const uint32_t *p = s.win(15 + vy0, b >> 2);
+    const uint32_t sh = (uint32_t)(b & 3) * 8u;
+    uint32_t lo[N], hi[N];   /* two accumulators per candidate: shorter chains */
+#pragma unroll
+    for (int k = 0; k < N; k++)
+        lo[k] = hi[k] = 0u;
+    auto row = [&](const uint32_t *q, uint32_t w[4]) {
+        const uint32_t x0 = q[0], x1 = q[1], x2 = q[2], x3 = q[3], x4 = q[4];
+        w[0] = __funnelshift_r(x0, x1, sh);
+        w[1] = __funnelshift_r(x1, x2, sh);
+        w[2] = __funnelshift_r(x2, x3, sh);
+        w[3] = __funnelshift_r(x3, x4, sh);
+    };
+    auto add = [&](int k, int r, const uint32_t w[4]) {
+        const uint4 c = *reinterpret_cast<const uint4 *>(s.cur(r, 0));
+        lo[k] = sad4(c.x, w[0], lo[k]);
+        hi[k] = sad4(c.y, w[1], hi[k]);
+        lo[k] = sad4(c.z, w[2], lo[k]);
+        hi[k] = sad4(c.w, w[3], hi[k]);
+    };
+    /* rows 0 .. N-2: candidates k <= R */
+#pragma unroll
+    for (int R = 0; R < N - 1; R++) {
+        uint32_t w[4];
+        row(p + R * WIN_PITCH_W, w);
+#pragma unroll
+        for (int k = 0; k <= R; k++)
+            add(k, R - k, w);
+    }
+    /* rows N-1 .. 15: every candidate */
+#pragma unroll 1
+    for (int R = N - 1; R < 16; R++) {
+        uint32_t w[4];
+        row(p + R * WIN_PITCH_W, w);
+#pragma unroll
+        for (int k = 0; k < N; k++)
+            add(k, R - k, w);
+    }
+    /* rows 16 .. 14+N: candidates k >= R - 15 */
+#pragma unroll
+    for (int R = 16; R < 15 + N; R++) {
+        uint32_t w[4];
+        row(p + R * WIN_PITCH_W, w);
+#pragma unroll
+        for (int k = R - 15; k < N; k++)
+            add(k, R - k, w);
+    }
+#pragma unroll
+    for (int k = 0; k < N; k++)
+        sad[k] = lo[k] + hi[k];
+}
+
 /* 4x4 Hadamard SATD, megpu_kernels.cuh:467-500 */
 __device__ __forceinline__ int32_t satd4x4(const int32_t d[16])
 {
@@ -381,19 +444,22 @@ __device__ __forceinline__ void motion_estimate(const StageBuf s, const h261b_se
      * limits is replaced by (0, 0) so no address leaves the window, and its
      * cost discarded (65535, as the reference marks skipped candidates) */
     if (S.me_mode == 1) {
+        /* columns of four vertically adjacent vectors: 31 columns x 8
+         * groups, the last group (vy 13..15) started at vy 12, which the
+         * group before holds too (a repeated key changes no minimum) */
         uint32_t best = FULL;
-        for (int c = lane; c < 31 * 31; c += 64) {
-            const int c1 = c + 32;
-            const bool has1 = c1 < 31 * 31;
-            const int ty0 = c / 31, tx0 = c - ty0 * 31, ty1 = (has1 ? c1 : c) / 31, tx1 = (has1 ? c1 : c) - ty1 * 31;
-            const int x0 = tx0 - 15, y0 = ty0 - 15, x1 = tx1 - 15, y1 = ty1 - 15;
-            const bool o0 = x0 >= lminx && x0 <= lmaxx && y0 >= lminy && y0 <= lmaxy;
-            const bool o1 = has1 && x1 >= lminx && x1 <= lmaxx && y1 >= lminy && y1 <= lmaxy;
-            uint32_t s0, s1;
-            sad16x16_pair(s, o0 ? x0 : 0, o0 ? y0 : 0, o1 ? x1 : 0, o1 ? y1 : 0, s0, s1);
-            best = min(best, ((o0 ? s0 : 65535u) << 10) | zorder(tx0, ty0));
-            if (has1)
-                best = min(best, ((o1 ? s1 : 65535u) << 10) | zorder(tx1, ty1));
+        for (int t = lane; t < 31 * 8; t += 32) {
+            const int gy = t / 31, tx = t - gy * 31;
+            const int x = tx - 15, y0 = min(-15 + 4 * gy, 12);
+            uint32_t sad[4];
+            sad16x16_column<4>(s, x, y0, sad);
+            const bool ox = x >= lminx && x <= lmaxx;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int y = y0 + k;
+                const bool ok = ox && y >= lminy && y <= lmaxy;
+                best = min(best, ((ok ? sad[k] : 65535u) << 10) | zorder(tx, y + 15));
+            }
         }
         best = __reduce_min_sync(FULL, best) & 1023u; /* Z-order index only */
         vx = (int)compact8(best) - 15;
@@ -418,19 +484,27 @@ __device__ __forceinline__ void motion_estimate(const StageBuf s, const h261b_se
         const int v1x = stage1_offset((int)compact8(best)), v1y = stage1_offset((int)compact8(best >> 1));
         s1x = (int8_t)v1x;
         s1y = (int8_t)v1y;
+        /* the 7x7 refinement as 28 vertical pairs, lanes 0-27: column tx,
+         * rows 2gy and 2gy+1 (row 7 of the last pair is past the grid).  A
+         * pair reaching past +-15 is computed from the nearest in-window
+         * rows and each vector takes its SAD from there; vectors outside
+         * the limits are discarded as before */
         best = FULL;
-        {
-            const int c = lane, c1 = lane + 32;
-            const bool has1 = c1 < 49;
-            const int ty0 = c / 7, tx0 = c - ty0 * 7, ty1 = (has1 ? c1 : c) / 7, tx1 = (has1 ? c1 : c) - ty1 * 7;
-            const int x0 = v1x + tx0 - 3, y0 = v1y + ty0 - 3, x1 = v1x + tx1 - 3, y1 = v1y + ty1 - 3;
-            const bool o0 = x0 >= lminx && x0 <= lmaxx && y0 >= lminy && y0 <= lmaxy;
-            const bool o1 = has1 && x1 >= lminx && x1 <= lmaxx && y1 >= lminy && y1 <= lmaxy;
-            uint32_t s0, s1;
-            sad16x16_pair(s, o0 ? x0 : 0, o0 ? y0 : 0, o1 ? x1 : 0, o1 ? y1 : 0, s0, s1);
-            best = min(best, ((o0 ? s0 : 65535u) << 10) | zorder(tx0, ty0));
-            if (has1)
-                best = min(best, ((o1 ? s1 : 65535u) << 10) | zorder(tx1, ty1));
+        if (lane < 28) {
+            const int gy = lane / 7, tx = lane - gy * 7;
+            const int x = v1x + tx - 3, y0 = v1y + 2 * gy - 3;
+            const int base = min(max(y0, -15), 14);
+            uint32_t sad[2];
+            sad16x16_column<2>(s, min(max(x, -15), 15), base, sad);
+            const bool ox = x >= lminx && x <= lmaxx;
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const int y = y0 + k, ty = 2 * gy + k;
+                const bool ok = ox && ty < 7 && y >= lminy && y <= lmaxy;
+                const uint32_t v = (y - base) == 0 ? sad[0] : sad[1];
+                if (ty < 7)
+                    best = min(best, ((ok ? v : 65535u) << 10) | zorder(tx, ty));
+            }
         }
         best = __reduce_min_sync(FULL, best) & 1023u;
         vx = v1x + (int)compact8(best) - 3;
