@@ -121,6 +121,7 @@ def core() -> ctypes.CDLL:
         lib.h261b_session_open.argtypes = [c_void_p, POINTER(SessionConfig), POINTER(c_int32)]
         lib.h261b_session_close.argtypes = [c_void_p, c_int32]
         lib.h261b_engine_reserve.argtypes = [c_void_p, POINTER(SessionConfig), c_int32]
+        lib.h261b_engine_wait_step.argtypes = [c_void_p, c_int64]
         lib.h261b_engine_reserve_step.argtypes = [c_void_p, POINTER(SessionConfig), c_int32]
         lib.h261b_session_submit.argtypes = [c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_int32]
         lib.h261b_session_submit_device.argtypes = [c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_int32]

@@ -10,12 +10,13 @@
  * one copy, runs one launch over the flat (session, MB) work list, and
  * brings the compact results of all sessions back with one copy.
  *
- * Pipelining: steps alternate between two CUDA streams and two sets of
- * arenas (by step parity).  Within a step the order is upload -> kernel ->
+ * Pipelining: steps rotate over NSLOT (3) slots, each with its CUDA stream
+ * and its set of arenas.  Within a step the order is upload -> kernel ->
  * download; across steps only the kernels are ordered (step k+1's kernel
  * waits for step k's, whose reconstructions are its references), so step
  * k+1's upload overlaps step k's kernel and step k's download overlaps step
- * k+1's kernel.  Results of step k stay readable until step k+2 is issued.
+ * k+1's kernel.  Results of step k stay readable until step k+3 is issued,
+ * so a caller can issue step k+1 while it has still to read step k-1.
  *
  * Tuning: when warps_per_cta is 0 the first steps try each launch shape on
  * live work (the results do not depend on it) and keep the fastest by CUDA
@@ -37,6 +38,11 @@
 #include "h261b_device.h"
 
 namespace h261b {
+
+/* steps in flight at once: step id uses slot id % NSLOT (its stream,
+ * arenas, events and graph), so the host can issue a step while the two
+ * before it still run and their results are still readable */
+constexpr int NSLOT = 3;
 
 static thread_local char g_err[512];
 
@@ -165,7 +171,7 @@ struct StepKey {
 struct StepGraph {
     cudaGraphExec_t exec = nullptr;
     StepKey key;
-    /* the signature of the last step launched directly on this parity: a
+    /* the signature of the last step launched directly on this slot: a
      * graph is captured only for a signature seen twice in a row, so that
      * steps whose sessions keep changing (one stream at a time, serving)
      * do not pay a capture each */
@@ -235,10 +241,10 @@ struct Session {
     int rec_cur = 0;               /* holds the latest reconstruction     */
     h261b_denoise_dev_t *dn = nullptr;
     size_t slot_bytes = 0;
-    /* bitstream: one device block per step parity (picture, MB scratch,
+    /* bitstream: one device block per step slot (picture, MB scratch,
      * positions, header plans, picture size) */
     bool bitstream = false;
-    uint8_t *bits_base[2] = { nullptr, nullptr };
+    uint8_t *bits_base[NSLOT] = {};
     h261b_bits_layout_t bits_lay = {};
     std::vector<uint8_t> bits_spill;   /* a picture the host arena missed */
     /* CBR rate control: its state and the mode decisions between the two
@@ -252,7 +258,7 @@ struct Session {
     size_t src_off = 0;
     const uint8_t *dev_src[3] = { nullptr, nullptr, nullptr };
     int32_t queued_quant = 0;
-    Result res[2];                 /* by step parity                      */
+    Result res[NSLOT];             /* by step slot                        */
 };
 
 } // namespace h261b
@@ -262,43 +268,43 @@ using namespace h261b;
 struct h261b_engine_s {
     h261b_engine_config_t cfg;
     int sm_count = 0;
-    cudaStream_t stream[2] = { nullptr, nullptr };
-    /* per parity: a side stream that records the events marking the encode
+    cudaStream_t stream[NSLOT] = {};
+    /* per slot: a side stream that records the events marking the encode
      * kernel's end, so that nothing sits between the encode kernel and the
      * bitstream kernel that depends on it (a programmatic dependent launch) */
-    cudaStream_t side[2] = { nullptr, nullptr };
-    cudaEvent_t fork_ev[2] = { nullptr, nullptr }, join_ev[2] = { nullptr, nullptr };
+    cudaStream_t side[NSLOT] = {};
+    cudaEvent_t fork_ev[NSLOT] = {}, join_ev[NSLOT] = {};
     DevicePool pool;
     std::vector<Session> sessions;
     int32_t open_count = 0;
     int64_t session_bytes = 0;
 
-    Mirror upload[2];          /* queued source pictures                  */
-    Mirror results[2];         /* mb info + levels of every session        */
-    Mirror desc[2];            /* session descriptors + work list           */
+    Mirror upload[NSLOT];      /* queued source pictures                  */
+    Mirror results[NSLOT];     /* mb info + levels of every session        */
+    Mirror desc[NSLOT];        /* session descriptors + work list           */
     size_t upload_used = 0;    /* bytes queued for the next step           */
     bool upload_checked = false;
-    int64_t next_step = 0;     /* id of the next step; parity = id & 1      */
+    int64_t next_step = 0;     /* id of the next step; slot = id % NSLOT    */
     int64_t done_step = -1;    /* every step up to this one has completed   */
-    cudaEvent_t h2d_done[2] = { nullptr, nullptr };
-    cudaEvent_t kernel_done[2] = { nullptr, nullptr };
-    cudaEvent_t step_done[2] = { nullptr, nullptr };
-    cudaEvent_t k_start[2] = { nullptr, nullptr }, k_end[2] = { nullptr, nullptr };
-    cudaEvent_t b_end[2] = { nullptr, nullptr };   /* after the bitstream kernel */
-    cudaEvent_t layout_done[2] = { nullptr, nullptr };   /* rate control inputs written */
+    cudaEvent_t h2d_done[NSLOT] = {};
+    cudaEvent_t kernel_done[NSLOT] = {};
+    cudaEvent_t step_done[NSLOT] = {};
+    cudaEvent_t k_start[NSLOT] = {}, k_end[NSLOT] = {};
+    cudaEvent_t b_end[NSLOT] = {};         /* after the bitstream kernel */
+    cudaEvent_t layout_done[NSLOT] = {};   /* rate control inputs written */
     /* timing of each phase of a step: begin, uploads done, kernels may
      * start (the previous step's encode is done), results downloaded */
-    cudaEvent_t t_begin[2] = { nullptr, nullptr }, t_h2d[2] = { nullptr, nullptr };
-    cudaEvent_t t_ready[2] = { nullptr, nullptr }, t_end[2] = { nullptr, nullptr };
+    cudaEvent_t t_begin[NSLOT] = {}, t_h2d[NSLOT] = {};
+    cudaEvent_t t_ready[NSLOT] = {}, t_end[NSLOT] = {};
     /* step arena bytes asked for by h261b_engine_reserve_step */
     size_t reserved_upload = 0, reserved_results = 0, reserved_desc = 0;
     /* the encode launches' work counters, two per stream (h261b_launch_step) */
     int32_t *sched_dev = nullptr;
-    bool step_bits_ran[2] = { false, false };
-    bool in_flight[2] = { false, false };
-    int64_t step_mbs[2] = { 0, 0 };   /* MB records of the step in each arena */
+    bool step_bits_ran[NSLOT] = {};
+    bool in_flight[NSLOT] = {};
+    int64_t step_mbs[NSLOT] = {};   /* MB records of the step in each arena */
     int64_t last_h2d = 0, last_d2h = 0;  /* bytes copied by the last step */
-    HostArena bits[2];         /* pictures written by the bitstream kernel */
+    HostArena bits[NSLOT];     /* pictures written by the bitstream kernel */
     size_t bits_want = 0;      /* capacity the arenas grow to              */
     /* slots of closed sessions, returned to the pool once the last step
      * that may use them (second field) has completed */
@@ -312,7 +318,7 @@ struct h261b_engine_s {
     std::vector<CopyJob> copy_jobs;
 
     /* graph replay of steps (use_graphs) */
-    StepGraph graph[2];
+    StepGraph graph[NSLOT];
     bool graphs_off = false;
     int64_t graph_captures = 0, graph_replays = 0;
 
@@ -360,7 +366,7 @@ extern "C" int64_t h261b_session_bytes(int32_t w, int32_t h)
 
 extern "C" int64_t h261b_session_bits_bytes(int32_t w, int32_t h)
 {
-    return 2 * (int64_t)align_up((size_t)h261b_bits_slot_bytes(w, h), 256);
+    return NSLOT * (int64_t)align_up((size_t)h261b_bits_slot_bytes(w, h), 256);
 }
 
 /* rate-control state and one picture's mode decisions */
@@ -403,7 +409,7 @@ static void reclaim(h261b_engine_t *e)
 
 static int sync_all(h261b_engine_t *e)
 {
-    for (int p = 0; p < 2; p++)
+    for (int p = 0; p < NSLOT; p++)
         H261B_CUDA_TRY(cudaStreamSynchronize(e->stream[p]));
     e->done_step = e->next_step - 1;
     reclaim(e);
@@ -436,7 +442,7 @@ extern "C" int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engin
     e->copier.reset(new CopyPool(copiers - 1));   /* the caller is one of them */
     cudaDeviceProp prop;
     bool ok = cudaGetDeviceProperties(&prop, cfg->device) == cudaSuccess && h261b_set_quant_table() == 0;
-    for (int p = 0; p < 2 && ok; p++) {
+    for (int p = 0; p < NSLOT && ok; p++) {
         ok = cudaStreamCreateWithFlags(&e->stream[p], cudaStreamNonBlocking) == cudaSuccess &&
              cudaStreamCreateWithFlags(&e->side[p], cudaStreamNonBlocking) == cudaSuccess &&
              cudaEventCreateWithFlags(&e->fork_ev[p], cudaEventDisableTiming) == cudaSuccess &&
@@ -450,8 +456,8 @@ extern "C" int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engin
              cudaEventCreate(&e->t_h2d[p]) == cudaSuccess && cudaEventCreate(&e->t_ready[p]) == cudaSuccess &&
              cudaEventCreate(&e->t_end[p]) == cudaSuccess;
     }
-    ok = ok && cudaMalloc(&e->sched_dev, 4 * sizeof(int32_t)) == cudaSuccess &&
-         cudaMemset(e->sched_dev, 0, 4 * sizeof(int32_t)) == cudaSuccess;
+    ok = ok && cudaMalloc(&e->sched_dev, 2 * NSLOT * sizeof(int32_t)) == cudaSuccess &&
+         cudaMemset(e->sched_dev, 0, 2 * NSLOT * sizeof(int32_t)) == cudaSuccess;
     if (!ok) {
         set_error("h261b_engine_create: device setup failed: %s", cudaGetErrorString(cudaGetLastError()));
         h261b_engine_destroy(e);
@@ -461,7 +467,7 @@ extern "C" int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engin
     if (cfg->bits_host_bytes > 0) {
         /* a configured host bitstream arena is allocated now, not by the
          * first steps */
-        for (int p = 0; p < 2; p++)
+        for (int p = 0; p < NSLOT; p++)
             if (e->bits[p].reserve(e->bits_want) != H261B_OK) {
                 h261b_engine_destroy(e);
                 return H261B_ERR_NOMEM;
@@ -501,10 +507,10 @@ extern "C" int h261b_engine_destroy(h261b_engine_t *e)
     cudaSetDevice(e->cfg.device);
     if (e->copier)
         e->copier->join();
-    for (int p = 0; p < 2; p++)
+    for (int p = 0; p < NSLOT; p++)
         if (e->stream[p])
             cudaStreamSynchronize(e->stream[p]);
-    for (int p = 0; p < 2; p++) {
+    for (int p = 0; p < NSLOT; p++) {
         e->graph[p].reset();
         e->upload[p].release();
         e->results[p].release();
@@ -599,8 +605,8 @@ extern "C" int h261b_session_open(h261b_engine_t *e, const h261b_session_config_
         uint8_t *b0 = base + h261b_session_bytes(c->width, c->height);
         s.bitstream = true;
         s.bits_lay = h261b_bits_layout(c->width, c->height);
-        s.bits_base[0] = b0;
-        s.bits_base[1] = b0 + sb;
+        for (int q = 0; q < NSLOT; q++)
+            s.bits_base[q] = b0 + q * sb;
     }
     h261b_rc_dev_t rc0;
     if (c->rate_control) {
@@ -630,9 +636,9 @@ extern "C" int h261b_session_open(h261b_engine_t *e, const h261b_session_config_
     h261b_denoise_dev_t dn0;
     memset(&dn0, 0, sizeof(dn0));
     dn0.denoise = c->denoise;
-    cudaStream_t st = e->stream[e->next_step & 1];
+    cudaStream_t st = e->stream[e->next_step % NSLOT];
     H261B_CUDA_TRY(cudaMemsetAsync(base, 0, 2 * s.lay.bytes, st));
-    for (int q = 0; q < 2 && s.bitstream; q++)
+    for (int q = 0; q < NSLOT && s.bitstream; q++)
         H261B_CUDA_TRY(cudaMemsetAsync(s.bits_base[q] + s.bits_lay.total, 0, 256, st));
     if (s.rc)
         H261B_CUDA_TRY(cudaMemcpyAsync(s.rc_dev, &rc0, sizeof(rc0), cudaMemcpyHostToDevice, st));
@@ -676,8 +682,8 @@ extern "C" int h261b_engine_reserve_step(h261b_engine_t *e, const h261b_session_
     e->reserved_results += k * (nmb * sizeof(h261b_mb_info_t) + sizeof(h261b_pic_info_t) + 32 +
                                 align_up(nmb * 384, 256)) + 1024;
     e->reserved_desc += k * (sizeof(h261b_session_dev_t) + nmb * sizeof(uint32_t)) + 1024;
-    for (int p = 0; p < 2; p++) {
-        const size_t keep = (p == (int)(e->next_step & 1) && e->upload_checked) ? e->upload_used : 0;
+    for (int p = 0; p < NSLOT; p++) {
+        const size_t keep = (p == (int)(e->next_step % NSLOT) && e->upload_checked) ? e->upload_used : 0;
         int rc = grow_arenas(e, p, e->reserved_upload, keep, e->reserved_results, e->reserved_desc);
         if (rc)
             return rc;
@@ -701,12 +707,12 @@ extern "C" int h261b_session_close(h261b_engine_t *e, int32_t id)
     return H261B_OK;
 }
 
-/* Grow the arenas of parity p to hold `up` upload bytes (the first `keep`
+/* Grow the arenas of slot p to hold `up` upload bytes (the first `keep`
  * of which are queued pictures that survive), `res` result bytes and `desc`
  * descriptor bytes.  Sized by what a step actually holds, not by every open
  * session, so that a server with thousands of open sessions and a few
  * pictures per step keeps small arenas; they grow by doubling, so a
- * growing load reallocates (and waits for the parity's stream) a few times
+ * growing load reallocates (and waits for the slot's stream) a few times
  * only. */
 static int grow_arenas(h261b_engine_t *e, int p, size_t up, size_t keep, size_t res, size_t desc)
 {
@@ -731,9 +737,9 @@ static int reserve_input(h261b_engine_t *e, Session *s, int32_t id, int32_t quan
         set_error("%s: session %d already has a queued picture", who, id);
         return H261B_ERR_STATE;
     }
-    const int p = (int)(e->next_step & 1);
+    const int p = (int)(e->next_step % NSLOT);
     if (!e->upload_checked) {
-        /* the copy that last read this pinned arena (two steps ago) must be
+        /* the copy that last read this pinned arena (NSLOT steps ago) must be
          * complete before the host writes into it */
         if (e->in_flight[p])
             H261B_CUDA_TRY(cudaEventSynchronize(e->h2d_done[p]));
@@ -769,7 +775,7 @@ extern "C" int h261b_session_submit(h261b_engine_t *e, int32_t id, const uint8_t
     int rc = reserve_input(e, s, id, quant, &off, "h261b_session_submit");
     if (rc)
         return rc;
-    uint8_t *dst = e->upload[e->next_step & 1].host + off;
+    uint8_t *dst = e->upload[e->next_step % NSLOT].host + off;
     const size_t ny = (size_t)s->w * s->h, nc = ny / 4;
     memcpy(dst + s->lay.off_y, y, ny);
     memcpy(dst + s->lay.off_cb, cb, nc);
@@ -792,7 +798,7 @@ extern "C" int h261b_engine_inputs(h261b_engine_t *e, int32_t n, const int32_t *
         }
     /* room for the whole batch at once: one reallocation at most */
     {
-        const int p = (int)(e->next_step & 1);
+        const int p = (int)(e->next_step % NSLOT);
         if (!e->upload_checked) {
             if (e->in_flight[p])
                 H261B_CUDA_TRY(cudaEventSynchronize(e->h2d_done[p]));
@@ -825,7 +831,7 @@ extern "C" int h261b_engine_inputs(h261b_engine_t *e, int32_t n, const int32_t *
         offsets[3 * i + 1] = (int64_t)(off + s->lay.off_cb);
         offsets[3 * i + 2] = (int64_t)(off + s->lay.off_cr);
     }
-    *staging = e->upload[e->next_step & 1].host;
+    *staging = e->upload[e->next_step % NSLOT].host;
     return H261B_OK;
 }
 
@@ -889,7 +895,7 @@ extern "C" int h261b_engine_step_records(h261b_engine_t *e, const h261b_mb_resul
         *count = 0;
         return H261B_OK;
     }
-    const int p = (int)(e->done_step & 1);
+    const int p = (int)(e->done_step % NSLOT);
     *records = (const h261b_mb_result_t *)e->results[p].host;
     *count = e->step_mbs[p];
     return H261B_OK;
@@ -909,7 +915,7 @@ extern "C" int h261b_session_input(h261b_engine_t *e, int32_t id, int32_t quant,
     int rc = reserve_input(e, s, id, quant, &off, "h261b_session_input");
     if (rc)
         return rc;
-    uint8_t *dst = e->upload[e->next_step & 1].host + off;
+    uint8_t *dst = e->upload[e->next_step % NSLOT].host + off;
     *y = dst + s->lay.off_y;
     *cb = dst + s->lay.off_cb;
     *cr = dst + s->lay.off_cr;
@@ -964,7 +970,8 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
         return H261B_ERR_ARG;
     cudaSetDevice(e->cfg.device);
     const int64_t id = e->next_step;
-    const int p = (int)(id & 1);
+    const int p = (int)(id % NSLOT);
+    const int prev = (int)((id + NSLOT - 1) % NSLOT);   /* the slot of step id - 1 */
     std::vector<int32_t> list;
     for (size_t i = 0; i < e->sessions.size(); i++)
         if (e->sessions[i].open && e->sessions[i].queued)
@@ -993,10 +1000,10 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
             return rc;
     }
     int rc;
-    /* arenas of this parity were last used by step id-2 */
-    if (e->in_flight[p] && id - 2 > e->done_step) {
+    /* arenas of this slot were last used by step id - NSLOT */
+    if (e->in_flight[p] && id - NSLOT > e->done_step) {
         H261B_CUDA_TRY(cudaEventSynchronize(e->step_done[p]));
-        e->done_step = id - 2;
+        e->done_step = id - NSLOT;
         reclaim(e);
     }
 
@@ -1137,7 +1144,7 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
         H261B_CUDA_TRY(cudaEventRecordWithFlags(e->t_h2d[p], st, rf));
         /* the previous step's reconstructions are this step's references */
         if (id > 0)
-            H261B_CUDA_TRY(cudaStreamWaitEvent(st, e->kernel_done[p ^ 1], wf));
+            H261B_CUDA_TRY(cudaStreamWaitEvent(st, e->kernel_done[prev], wf));
         H261B_CUDA_TRY(cudaEventRecordWithFlags(e->t_ready[p], st, rf));
         H261B_CUDA_TRY(cudaEventRecordWithFlags(e->k_start[p], st, rf));
         int32_t *sched = e->sched_dev + 2 * p;
@@ -1145,9 +1152,11 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
         if (lr == 0 && n_rc) {
             /* rate-controlled sessions: the picture QUANT from this
              * picture's costs and the previous picture's size (written by
-             * the previous step's layout kernel), then their encode */
-            if (id > 0)
-                H261B_CUDA_TRY(cudaStreamWaitEvent(st, e->layout_done[p ^ 1], wf));
+             * the layout kernel of the step that held it), then their
+             * encode.  That step is one of the other slots' latest (a
+             * session may skip steps) or older, on this stream. */
+            for (int q = 1; q < NSLOT && q <= id; q++)
+                H261B_CUDA_TRY(cudaStreamWaitEvent(st, e->layout_done[(id + NSLOT - q) % NSLOT], wf));
             lr = h261b_launch_ratectrl(desc_dev, (int32_t)n, st);
             if (lr == 0)
                 lr = h261b_launch_step(desc_dev, work_dev + rc_begin, n_work - rc_begin,
@@ -1182,15 +1191,15 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
     };
 
     /* Steps whose launches look the same (sizes, arena addresses, launch
-     * shape) replay one CUDA graph per parity: the descriptor and work-list
+     * shape) replay one CUDA graph per slot: the descriptor and work-list
      * contents differ, but they are data in pinned memory that the graph's
      * upload copies.  A signature is captured the second time in a row it
-     * comes on its parity.  Tuning steps, an engine's first step and engines
+     * comes on its slot.  Tuning steps, an engine's first step and engines
      * with use_graphs = 0 launch directly. */
     const StepKey key = { dm.host, dm.dev, um.host, um.dev, rm.host, rm.dev, bits_dev_or_null(e, p, n_bits),
                           n_bits ? e->bits[p].cap : 0, desc_off, work_off, desc_bytes, upload_bytes, ssd_base,
                           d2h, (int64_t)n, n_work, rc_begin, n_rc, n_ssd ? 1 : 0, warps, ctas, phases,
-                          id > 0 ? 1 : 0 };
+                          (int32_t)std::min<int64_t>(id, NSLOT - 1) };
     StepGraph &gr = e->graph[p];
     const bool repeated = gr.has_last_direct && gr.last_direct == key;
     const bool capturable = e->cfg.use_graphs && !e->graphs_off && !tuning && id > 0;
@@ -1275,7 +1284,7 @@ static int wait_step(h261b_engine_t *e, int64_t id)
 {
     if (id < 0 || id <= e->done_step)
         return H261B_OK;
-    H261B_CUDA_TRY(cudaEventSynchronize(e->step_done[id & 1]));
+    H261B_CUDA_TRY(cudaEventSynchronize(e->step_done[id % NSLOT]));
     e->done_step = id;
     reclaim(e);
     return H261B_OK;
@@ -1287,6 +1296,22 @@ extern "C" int h261b_engine_sync(h261b_engine_t *e)
     if (!e)
         return H261B_ERR_ARG;
     return wait_step(e, e->next_step - 1);
+}
+
+extern "C" int h261b_engine_wait_step(h261b_engine_t *e, int64_t step)
+{
+    clear_error();
+    if (!e)
+        return H261B_ERR_ARG;
+    if (step >= e->next_step) {
+        set_error("h261b_engine_wait_step: step %lld has not been issued", (long long)step);
+        return H261B_ERR_STATE;
+    }
+    if (step < e->next_step - NSLOT) {
+        set_error("h261b_engine_wait_step: step %lld is older than the steps in flight", (long long)step);
+        return H261B_ERR_STATE;
+    }
+    return wait_step(e, step);
 }
 
 extern "C" int h261b_engine_wait_previous(h261b_engine_t *e)
@@ -1311,7 +1336,7 @@ extern "C" int h261b_session_result(h261b_engine_t *e, int32_t id, h261b_frame_r
         set_error("h261b_session_result: no completed step for session %d (wait for a step first)", id);
         return H261B_ERR_STATE;
     }
-    const int p = (int)(best->step & 1);
+    const int p = (int)(best->step % NSLOT);
     const Mirror &rm = e->results[p];
     out->frame_index = best->frame;
     out->frame_type = best->type;
@@ -1369,7 +1394,7 @@ extern "C" int h261b_engine_step_bits(h261b_engine_t *e, int64_t *bytes, int32_t
         *pictures = 0;
     if (e->done_step < 0)
         return H261B_OK;
-    const int p = (int)(e->done_step & 1);
+    const int p = (int)(e->done_step % NSLOT);
     const Mirror &rm = e->results[p];
     for (const Session &s : e->sessions) {
         const Result &r = s.res[p];
@@ -1437,7 +1462,7 @@ extern "C" int h261b_engine_last_kernel_ms(h261b_engine_t *e, float *ms)
 {
     if (!e || !ms || e->next_step == 0)
         return H261B_ERR_ARG;
-    const int p = (int)((e->next_step - 1) & 1);
+    const int p = (int)((e->next_step - 1) % NSLOT);
     H261B_CUDA_TRY(cudaEventSynchronize(e->k_end[p]));
     H261B_CUDA_TRY(cudaEventElapsedTime(ms, e->k_start[p], e->k_end[p]));
     return H261B_OK;
@@ -1456,7 +1481,7 @@ extern "C" int h261b_engine_last_bits_ms(h261b_engine_t *e, float *ms)
 {
     if (!e || !ms || e->next_step == 0)
         return H261B_ERR_ARG;
-    const int p = (int)((e->next_step - 1) & 1);
+    const int p = (int)((e->next_step - 1) % NSLOT);
     *ms = 0.f;
     if (!e->step_bits_ran[p])
         return H261B_OK;
@@ -1474,7 +1499,7 @@ extern "C" int h261b_engine_step_timing(h261b_engine_t *e, h261b_step_timing_t *
         set_error("h261b_engine_step_timing: no step has completed");
         return H261B_ERR_STATE;
     }
-    const int p = (int)(e->done_step & 1);
+    const int p = (int)(e->done_step % NSLOT);
     float a = 0, b = 0, c = 0, d = 0, f = 0;
     H261B_CUDA_TRY(cudaEventElapsedTime(&a, e->t_begin[p], e->t_h2d[p]));
     H261B_CUDA_TRY(cudaEventElapsedTime(&b, e->t_h2d[p], e->t_ready[p]));
@@ -1504,7 +1529,7 @@ extern "C" int h261b_engine_step_pictures(h261b_engine_t *e, int32_t cap, h261b_
         *arena_bytes = 0;
     if (e->done_step < 0)
         return H261B_OK;
-    const int p = (int)(e->done_step & 1);
+    const int p = (int)(e->done_step % NSLOT);
     const Mirror &rm = e->results[p];
     int64_t span = 0;
     int32_t n = 0;

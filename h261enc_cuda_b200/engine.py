@@ -158,7 +158,8 @@ class Engine:
 
     def step_records(self):
         """(step number, MB records of every session that step encoded) for
-        the latest completed step; a view valid until the step after next."""
+        the latest completed step; a view valid until the third step after it is
+        issued."""
         ptr, count, step = ctypes.c_void_p(), ctypes.c_int64(), ctypes.c_int64()
         check(_lib.core().h261b_engine_step_records(self._h, ctypes.byref(ptr), ctypes.byref(count),
                                                     ctypes.byref(step)), "h261b_engine_step_records")
@@ -178,6 +179,11 @@ class Engine:
 
     def sync(self) -> None:
         check(_lib.core().h261b_engine_sync(self._h), "h261b_engine_sync")
+
+    def wait_step(self, step: int) -> None:
+        """Wait for step number ``step`` (0, 1, ... in issue order), one of
+        the last three issued; its results become the latest readable."""
+        check(_lib.core().h261b_engine_wait_step(self._h, step), "h261b_engine_wait_step")
 
     def wait_previous(self) -> None:
         """Wait for the step before the last one issued."""

@@ -166,9 +166,14 @@ int h261b_session_submit_device(h261b_engine_t *e, int32_t session_id, const uin
 int h261b_engine_step(h261b_engine_t *e);
 /* Wait for the last step issued / for the one before it (so the host can
  * read step k's results while step k+1 runs).  A step's results stay
- * readable until the step after next is issued. */
+ * readable until the third step after it is issued. */
 int h261b_engine_sync(h261b_engine_t *e);
 int h261b_engine_wait_previous(h261b_engine_t *e);
+/* Wait for step number `step` (steps are numbered 0, 1, ... in issue order)
+ * to complete; its results are then the latest readable ones.  With two
+ * steps issued ahead, a caller reads step k-2 while k-1 and k run.  Only
+ * the steps still in flight (the last three issued) can be waited for. */
+int h261b_engine_wait_step(h261b_engine_t *e, int64_t step);
 
 /* per-macroblock result of a step (16 bytes) */
 typedef struct {
@@ -205,14 +210,15 @@ typedef struct {
 } h261b_frame_result_t;
 
 /* Results of the latest completed step that encoded this session (pointers
- * stay valid until the step after next is issued). */
+ * stay valid until the third step after that one is issued). */
 int h261b_session_result(h261b_engine_t *e, int32_t session_id, h261b_frame_result_t *out);
 
 /* The macroblock records of the latest completed step as one array: the
  * records of every session the step encoded, session after session in
  * ascending session id (each session's h261b_session_result().mbs points
  * into it).  *step receives the step's number (0, 1, ...), -1 and *count 0
- * when no step has completed.  Valid until the step after next is issued. */
+ * when no step has completed.  Valid until the third step after it is
+ * issued. */
 int h261b_engine_step_records(h261b_engine_t *e, const h261b_mb_result_t **records, int64_t *count,
                               int64_t *step);
 
@@ -235,7 +241,8 @@ typedef struct {
  * ascending session id: up to cap entries into out, *count = all of them.
  * *arena / *arena_bytes: the host arena holding them (each picture on a
  * 16-byte boundary) and the bytes of it in use, for callers that move a
- * step's output in one copy.  Valid until the step after next is issued. */
+ * step's output in one copy.  Valid until the third step after it is
+ * issued. */
 int h261b_engine_step_pictures(h261b_engine_t *e, int32_t cap, h261b_picture_t *out, int32_t *count,
                                const uint8_t **arena, int64_t *arena_bytes);
 
