@@ -424,11 +424,11 @@ def ours(args, world, rank, local, dist):
         torch.cuda.synchronize()
         return time.perf_counter() - t0, lat
 
-    lat_steps = min(args.steps, 100)
-    _, lat = pipeline(1, lat_steps)
-    h2d = d2h = 0
     e2e_wall, e2e_lat = pipeline(2, args.steps)
     e2e_s = shard.max_over_ranks(e2e_wall, dist, f"cuda:{local}")
+    e2e_h2d, e2e_d2h = h2d, d2h
+    _, lat = pipeline(1, min(args.steps, 100))
+    h2d, d2h = e2e_h2d, e2e_d2h
     e2e = mb_per_step * args.steps * world / e2e_s
     h2d //= args.steps
     d2h //= args.steps
