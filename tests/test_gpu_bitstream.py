@@ -2,6 +2,7 @@
 reference's.  Pinned against the golden fixtures (per-picture SHA-256 of the
 bitstream the reference produced on a B200) and against the oracle's
 restatement of the reference writers on the engine's own records."""
+import ctypes
 import glob
 import json
 import os
@@ -164,6 +165,43 @@ def test_rate_control_mixed_batch_pipelined_matches_oracle(gpu):
     for k in range(len(specs)):
         assert quants[k] == list(want[k][2]), f"session {k}: QUANTs {quants[k]} vs {list(want[k][2])}"
         assert got[k] == want[k][0], f"session {k}: bitstream"
+
+
+def test_rate_control_skipping_steps_two_behind_matches_oracle(gpu):
+    """CBR sessions that skip steps, with three steps in flight and the host
+    reading two behind: a session's rate control reads the size of its
+    previous picture, which may be two steps back on another stream, and
+    every stream still equals the oracle's frame loop."""
+    specs = [(352, 288, 256000, 51, 1), (176, 144, 64000, 52, 2), (176, 144, 96000, 53, 3)]
+    steps = 12
+    clips = [synth.clip(1 if w == 352 else 2, w, h, seed, steps) for (w, h, b, seed, every) in specs]
+    got = [b"" for _ in specs]
+    used = [0 for _ in specs]
+    with Engine(warps_per_cta=4, levels_to_host=0) as e:
+        sids = [e.open(w, h, 10, bitstream=1, rate_control=1, bitrate=b) for (w, h, b, _, _) in specs]
+
+        def read(k):
+            e.wait_step(k)
+            pics, _ = e.step_pictures(8)
+            for p in pics:
+                j = sids.index(int(p["session_id"]))
+                assert p["status"] in (0, 1)
+                got[j] += (ctypes.string_at(int(p["bits"]), int(p["bytes"])) if p["status"] == 0
+                           else e.result(int(p["session_id"]), copy=False).bits)
+
+        for k in range(steps):
+            live = [j for j, spec in enumerate(specs) if k % spec[4] == 0]
+            e.submit_frames([sids[j] for j in live], [clips[j][used[j]] for j in live])
+            for j in live:
+                used[j] += 1
+            e.step()
+            if k >= 2:
+                read(k - 2)
+        read(steps - 2)
+        read(steps - 1)
+    for j, (w, h, b, _, _) in enumerate(specs):
+        want = O.encode_stream(clips[j][:used[j]], w, h, quant=0, bitrate=b)[0]
+        assert got[j] == want, f"session {j}: bitstream"
 
 
 def test_rate_control_needs_bitstream(gpu):
