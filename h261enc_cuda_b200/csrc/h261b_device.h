@@ -115,7 +115,8 @@ typedef struct {
                                      H261B_VLC_MB_WORDS words apart          */
     int32_t *vlc_pos;             /* per MB: bit position in the picture     */
     uint32_t *vlc_plan;           /* per MB: header fields                   */
-    int32_t *vlc_total;           /* [0] picture bits, [1] status            */
+    int32_t *vlc_total;           /* [0] picture bits, [1] status, [2] host
+                                     arena offset, [3] MBs packed            */
     /* CBR sessions: the step's first encode launch runs search and mode
      * decision (into md_out, costs summed into rc), the rate control picks
      * the picture QUANT, a second launch encodes (md_in = md_out) */
@@ -148,15 +149,15 @@ int h261b_set_quant_table(void);
 /* the picture QUANT of every session with rc (one thread per session) */
 int h261b_launch_ratectrl(h261b_session_dev_t *sessions_dev, int32_t n_sessions, void *stream);
 
-/* the bitstream of every work item's session that has bits_out: four
- * launches (coefficient codes and packing over the step's work list,
- * layout and the host copy per session);
+/* the bitstream of every work item's session that has bits_out: three
+ * launches (coefficient codes and packing over the step's work list, the
+ * layout per session; the CTA that packs a picture's last MBs copies it);
  * the picture ends in bits_out and in the host arena (device-mapped pinned
  * memory, host_cap bytes) at an offset drawn from step->host_used */
 int h261b_launch_bitstream(h261b_session_dev_t *sessions_dev, int32_t n_sessions, const uint32_t *work_dev,
                            int32_t n_work, h261b_step_dev_t *step, uint8_t *host_arena_dev, int64_t host_cap,
                            int32_t sm_count, void *stream, void *layout_done_event);
-/* device bytes per step parity a w x h session's bitstream needs: picture
+/* device bytes per step slot a w x h session's bitstream needs: picture
  * bytes, MB scratch and offsets (0: no bitstream for this size), and where
  * each part starts in that block */
 int64_t h261b_bits_slot_bytes(int32_t w, int32_t h);
