@@ -285,25 +285,31 @@ class Runner:
 
     def __init__(self, engine, streams, pools):
         self.e, self.streams, self.pools = engine, streams, pools
-        self.sids = [engine.open(s.width, s.height, s.quant, bitstream=1) for s in streams]
-        self.pos = [0] * len(streams)
+        from h261enc_cuda_b200 import workloads
+        self.sids = np.array([engine.open(s.width, s.height, s.quant, bitstream=1) for s in streams], np.int32)
+        self.pos = np.zeros(len(streams), np.int64)
+        self.length = np.array([s.length for s in streams], np.int64)
         self.queued = 0            # steps queued so far
         self.ending = []           # (session, step holding its last picture)
         # host pictures: one contiguous (clip, W*H*3/2) array per stream
         self.base = np.array([p[1].ctypes.data for p in pools], np.uint64)
         self.fbytes = np.array([p[1].shape[1] for p in pools], np.uint64)
         self.ny = np.array([s.width * s.height for s in streams], np.uint64)
+        # clip picture of every position of one forwards-backwards period
+        self.period = max(2 * CLIP_LEN - 2, 1)
+        self.index = np.array([workloads.clip_index(k, CLIP_LEN) for k in range(self.period)], np.uint64)
 
     def _advance(self):
-        from h261enc_cuda_b200 import workloads
-        idx = np.empty(len(self.streams), np.uint64)
-        for k, s in enumerate(self.streams):
-            if self.pos[k] >= s.length:
-                self.ending.append((self.sids[k], self.queued - 1))
+        """The clip picture each stream sends next (array ops: the call sits
+        on the host's per-step path)."""
+        if (self.pos >= self.length).any():
+            for k in np.flatnonzero(self.pos >= self.length):
+                s = self.streams[k]
+                self.ending.append((int(self.sids[k]), self.queued - 1))
                 self.sids[k] = self.e.open(s.width, s.height, s.quant, bitstream=1)
                 self.pos[k] = 0
-            idx[k] = workloads.clip_index(self.pos[k], CLIP_LEN)
-            self.pos[k] += 1
+        idx = self.index[self.pos % self.period]
+        self.pos += 1
         self.queued += 1
         return idx
 
@@ -320,7 +326,7 @@ class Runner:
     def queue_device(self):
         idx = self._advance()
         for k, sid in enumerate(self.sids):
-            self.e.submit_device(sid, *self.pools[k][2][int(idx[k])])
+            self.e.submit_device(int(sid), *self.pools[k][2][int(idx[k])])
 
     def queue_host(self, wait=True):
         """The next picture of every stream from host memory, in one call
@@ -413,10 +419,11 @@ def ours(args, world, rank, local, dist):
         for it in range(steps):
             issued.append(time.perf_counter())
             eng.step()
-            b_in, b_out = eng.last_copy_bytes()
-            h2d, d2h = h2d + b_in, d2h + b_out
+            # the next step's pictures start copying at once
             if it + 1 < steps:
                 run.queue_host(wait=False)
+            b_in, b_out = eng.last_copy_bytes()
+            h2d, d2h = h2d + b_in, d2h + b_out
             if it >= lag:
                 consume(it - lag)
         for k in range(max(0, steps - lag), steps):
