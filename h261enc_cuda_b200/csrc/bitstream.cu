@@ -508,7 +508,10 @@ __global__ void __launch_bounds__(VLC_THREADS) pack_kernel(const h261b_session_d
     __shared__ int done[PACK_DONE_MAX];
     __shared__ int n_done;
     pdl_launch_dependents();
-    const int lane = threadIdx.x & 31;
+    /* each half-warp packs every other MB of the warp's range, so that the
+     * two MBs' chains of dependent loads overlap */
+    const int lane = threadIdx.x & 31, half = lane >> 4, hl = lane & 15;
+    const unsigned hmask = 0xFFFFu << (16 * half);
     if (threadIdx.x == 0)
         n_done = 0;
     __syncthreads();
@@ -516,29 +519,29 @@ __global__ void __launch_bounds__(VLC_THREADS) pack_kernel(const h261b_session_d
     warp_range(n_work, lo, hi);
     pdl_wait();   /* the layout kernel's positions */
     int run_s = -1, run_n = 0;
-    /* the warp's finished MBs of picture run_s: published once the warp
+    /* the half-warp's finished MBs of picture run_s: published once it
      * moves on; the publication that completes the picture queues its copy */
     auto publish = [&]() {
         if (run_n == 0)
             return;
         const h261b_session_dev_t &P = sessions[run_s];
         __threadfence();   /* this lane's words before the count */
-        __syncwarp();
+        __syncwarp(hmask);
         int k = -1;
-        if (lane == 0 && atomicAdd(&P.vlc_total[3], run_n) + run_n == P.mbw * P.mbh) {
+        if (hl == 0 && atomicAdd(&P.vlc_total[3], run_n) + run_n == P.mbw * P.mbh) {
             k = atomicAdd(&n_done, 1);
             if (k < PACK_DONE_MAX)
                 done[k] = run_s;
         }
-        k = __shfl_sync(FULL, k, 0);
+        k = __shfl_sync(hmask, k, 16 * half);
         if (k >= PACK_DONE_MAX) {
-            /* the CTA's list is full: this warp copies the picture now */
+            /* the CTA's list is full: this half-warp copies the picture now */
             __threadfence();
-            copy_picture(P, host_arena, lane, 32);
+            copy_picture(P, host_arena, hl, 16);
         }
         run_n = 0;
     };
-    for (int w = lo; w < hi; w++) {
+    for (int w = lo + half; w < hi; w += 2) {
         const uint32_t item = work[w];
         const int sidx = (int)(item >> 12);
         const h261b_session_dev_t &S = sessions[sidx];
@@ -567,17 +570,17 @@ __global__ void __launch_bounds__(VLC_THREADS) pack_kernel(const h261b_session_d
         const int cbp = coded_blocks(r);
         /* the header as one MSB-first value of at most 57 bits */
         uint64_t hv;
-        int hl;
+        int hbits;
         {
             const uint16_t e = c_vlc_mba[addr];
             hv = e & 0xFF;
-            hl = e >> 8;
+            hbits = e >> 8;
             const int ml = c_vlc_mtype_len[mt];
             hv = (hv << ml) | 1u;
-            hl += ml;
+            hbits += ml;
             if (mq) {
                 hv = (hv << 5) | (uint32_t)r.quant;
-                hl += 5;
+                hbits += 5;
             }
             if (!intra && (r.flags & H261B_MB_MC)) {
                 uint32_t cx, cy;
@@ -585,26 +588,26 @@ __global__ void __launch_bounds__(VLC_THREADS) pack_kernel(const h261b_session_d
                 mvd_code(dx, cx, lx);
                 mvd_code(dy, cy, ly);
                 hv = (((hv << lx) | cx) << ly) | cy;
-                hl += lx + ly;
+                hbits += lx + ly;
             }
             if (!intra && cbp) {
                 const uint16_t e2 = c_vlc_cbp[cbp];
                 hv = (hv << (e2 >> 8)) | (e2 & 0xFF);
-                hl += e2 >> 8;
+                hbits += e2 >> 8;
             }
         }
-        if (lane == 0) {
-            if (hl > 32) {
-                put_bits_pic(S.bits_out, words, pos, (uint32_t)(hv >> 32), hl - 32, oob);
-                put_bits_pic(S.bits_out, words, pos + (hl - 32), (uint32_t)hv, 32, oob);
+        if (hl == 0) {
+            if (hbits > 32) {
+                put_bits_pic(S.bits_out, words, pos, (uint32_t)(hv >> 32), hbits - 32, oob);
+                put_bits_pic(S.bits_out, words, pos + (hbits - 32), (uint32_t)hv, 32, oob);
             } else {
-                put_bits_pic(S.bits_out, words, pos, (uint32_t)hv, hl, oob);
+                put_bits_pic(S.bits_out, words, pos, (uint32_t)hv, hbits, oob);
             }
         }
         /* the coefficient bits, shifted into place */
         const int nbits = r.coef_bits;
         if (nbits > 0) {
-            const int64_t q = pos + hl;
+            const int64_t q = pos + hbits;
             const int sh = (int)(q & 31);
             const int64_t w0 = q >> 5;
             const int nout = (sh + nbits + 31) >> 5, nin = (nbits + 31) >> 5;
@@ -612,7 +615,7 @@ __global__ void __launch_bounds__(VLC_THREADS) pack_kernel(const h261b_session_d
             if (w0 < 0 || w0 + nout > words || nin > MB_WORDS) {
                 oob = 1;
             } else {
-                for (int i = lane; i < nout; i += 32) {
+                for (int i = hl; i < nout; i += 16) {
                     const uint32_t hi = i < nin ? src[i] : 0u;
                     const uint32_t lo = i > 0 ? src[i - 1] : 0u;
                     const uint32_t x = sh ? ((hi >> sh) | (lo << (32 - sh))) : hi;
@@ -624,7 +627,7 @@ __global__ void __launch_bounds__(VLC_THREADS) pack_kernel(const h261b_session_d
                 }
             }
         }
-        if (__any_sync(FULL, oob) && lane == 0)
+        if (__any_sync(hmask, oob) && hl == 0)
             atomicExch(&S.vlc_total[1], H261B_BITS_MISMATCH);
     }
     publish();
