@@ -32,6 +32,7 @@ collective on the data path); rank 0 prints one JSON line.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -361,6 +362,12 @@ def ours(args, world, rank, local, dist):
         eng.sync()
         run.retire(run.queued - 1)
 
+    # the timed loops allocate no reference cycles: a full collection, which
+    # pauses the host for tens of milliseconds, would only add host stalls
+    gc_was_on = gc.isenabled()
+    gc.collect()
+    gc.disable()
+
     # ---- value: device-resident pictures, L2 flushed, the step's two
     # kernels (encode, bitstream) timed with CUDA events on its stream
     if dist:
@@ -461,6 +468,8 @@ def ours(args, world, rank, local, dist):
     single_s = time.perf_counter() - t0
     eng1.destroy()
     single = single_mbs / single_s
+    if gc_was_on:
+        gc.enable()
 
     if rank != 0:
         if dist:

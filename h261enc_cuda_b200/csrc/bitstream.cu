@@ -23,13 +23,13 @@
  *           flags; MB sizes, a scan over the GOB and one over the GOBs give
  *           every macroblock's position; the picture is cleared and gets its
  *           picture and GOB headers.
- *   pack    every coded macroblock writes its header and shifts its bit
- *           string into place; a macroblock's first and last word can be
- *           shared with its neighbours and are ORed in with atomics.  Warps
- *           count the MBs they finish per picture; the CTA whose count
- *           completes a picture copies it into the host arena (mapped
- *           pinned memory) at the offset layout drew with one atomic, and
- *           writes its record.
+ *   pack    every coded macroblock (one per half-warp) writes its header and
+ *           shifts its bit string into place; a macroblock's first and last
+ *           word can be shared with its neighbours and are ORed in with
+ *           atomics.  Half-warps count the MBs they finish per picture; the
+ *           CTA whose count completes a picture copies it into the host
+ *           arena (mapped pinned memory) at the offset layout drew with one
+ *           atomic, and writes its record.
  *
  * All three are programmatic dependent launches: the kernel before each
  * one (the encode kernel, codes, layout) lets it launch as soon as its own
