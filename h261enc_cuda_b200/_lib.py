@@ -125,6 +125,8 @@ def core() -> ctypes.CDLL:
         lib.h261b_engine_reserve_step.argtypes = [c_void_p, POINTER(SessionConfig), c_int32]
         lib.h261b_session_submit.argtypes = [c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_int32]
         lib.h261b_session_submit_device.argtypes = [c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_int32]
+        lib.h261b_engine_submit_device_batch.argtypes = [c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
+                                                         c_void_p]
         lib.h261b_measure_sad_peak.argtypes = [c_int32, POINTER(ctypes.c_double)]
         lib.h261b_session_input.argtypes = [c_void_p, c_int32, c_int32, POINTER(POINTER(c_uint8)),
                                             POINTER(POINTER(c_uint8)), POINTER(POINTER(c_uint8))]

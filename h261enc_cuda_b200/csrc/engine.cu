@@ -946,6 +946,51 @@ extern "C" int h261b_session_submit_device(h261b_engine_t *e, int32_t id, const 
     return H261B_OK;
 }
 
+extern "C" int h261b_engine_submit_device_batch(h261b_engine_t *e, int32_t n, const int32_t *ids,
+                                                const uint8_t *const *y, const uint8_t *const *cb,
+                                                const uint8_t *const *cr, const int32_t *quants)
+{
+    clear_error();
+    if (!e || n < 0 || (n > 0 && (!ids || !y || !cb || !cr))) {
+        set_error("h261b_engine_submit_device_batch: bad arguments");
+        return H261B_ERR_ARG;
+    }
+    /* all or nothing: every picture is checked before any is queued */
+    std::vector<int32_t> order(ids, ids + n);
+    std::sort(order.begin(), order.end());
+    if (std::adjacent_find(order.begin(), order.end()) != order.end()) {
+        set_error("h261b_engine_submit_device_batch: a session appears twice");
+        return H261B_ERR_ARG;
+    }
+    for (int32_t i = 0; i < n; i++) {
+        const Session *s = get_session(e, ids[i]);
+        const int32_t q = quants ? quants[i] : 0;
+        if (!s || !y[i] || !cb[i] || !cr[i] || q > 31) {
+            set_error("h261b_engine_submit_device_batch: picture %d: bad session, plane or QUANT", i);
+            return H261B_ERR_ARG;
+        }
+        if (((uintptr_t)y[i] & 15) || ((uintptr_t)cb[i] & 7) || ((uintptr_t)cr[i] & 7)) {
+            set_error("h261b_engine_submit_device_batch: picture %d: planes must be 16 (Y) and 8 (Cb, Cr) byte "
+                      "aligned", i);
+            return H261B_ERR_ARG;
+        }
+        if (s->queued) {
+            set_error("h261b_engine_submit_device_batch: session %d already has a queued picture", ids[i]);
+            return H261B_ERR_STATE;
+        }
+    }
+    for (int32_t i = 0; i < n; i++) {
+        Session &s = e->sessions[(size_t)ids[i]];
+        const int32_t q = quants ? quants[i] : 0;
+        s.dev_src[0] = y[i];
+        s.dev_src[1] = cb[i];
+        s.dev_src[2] = cr[i];
+        s.queued = true;
+        s.queued_quant = q > 0 ? q : 0;
+    }
+    return H261B_OK;
+}
+
 static int next_launch_shape(h261b_engine_t *e, int *warps, int *ctas)
 {
     if (!e->tuned && e->tune_next < e->tune_cands.size()) {

@@ -136,6 +136,17 @@ class Engine:
         arena = np.ctypeslib.as_array((ctypes.c_uint8 * size).from_address(base.value))
         return arena, offs
 
+    def submit_device_batch(self, sids, y_ptrs, cb_ptrs, cr_ptrs, quants=None) -> None:
+        """``submit_device`` for every session of ``sids`` in one call: device
+        plane addresses as uint64 arrays; all or nothing."""
+        sids = np.ascontiguousarray(sids, np.int32)
+        ptrs = [np.ascontiguousarray(a, np.uint64) for a in (y_ptrs, cb_ptrs, cr_ptrs)]
+        q = None if quants is None else np.ascontiguousarray(quants, np.int32)
+        check(_lib.core().h261b_engine_submit_device_batch(self._h, sids.size, sids.ctypes.data, ptrs[0].ctypes.data,
+                                                           ptrs[1].ctypes.data, ptrs[2].ctypes.data,
+                                                           None if q is None else q.ctypes.data),
+              "h261b_engine_submit_device_batch")
+
     def submit_batch(self, sids, y_ptrs, cb_ptrs, cr_ptrs, quants=None, wait: bool = True) -> None:
         """Queue one host picture for each of ``sids``: plane addresses as
         uint64 arrays (packed planes, e.g. ``frame.ctypes.data`` and the

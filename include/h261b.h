@@ -160,6 +160,14 @@ int h261b_engine_submit_batch_async(h261b_engine_t *e, int32_t n, const int32_t 
 int h261b_session_submit_device(h261b_engine_t *e, int32_t session_id, const uint8_t *y, const uint8_t *cb,
                                 const uint8_t *cr, int32_t quant);
 
+/* h261b_session_submit_device for n sessions in one call: picture i of
+ * session ids[i] at device planes y[i], cb[i], cr[i] with QUANT quants[i]
+ * (quants may be NULL).  All or nothing: nothing is queued when any picture
+ * is refused (a session named twice, not open or already queued, a NULL or
+ * misaligned plane, QUANT above 31). */
+int h261b_engine_submit_device_batch(h261b_engine_t *e, int32_t n, const int32_t *ids, const uint8_t *const *y,
+                                     const uint8_t *const *cb, const uint8_t *const *cr, const int32_t *quants);
+
 /* Encode the queued picture of every session that has one (one frame-step).
  * Returns the number of pictures encoded (>= 0) or a negative status.  The
  * call is asynchronous; results become readable after h261b_engine_sync(). */

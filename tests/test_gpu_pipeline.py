@@ -1,9 +1,10 @@
-"""The engine's pipelined use: steps issued back to back on its two streams,
-the host reading step k-1 while step k runs, streams ending and new sessions
-taking their place without a drain, and the ways of queueing host pictures
-(one copy per call, the batched copy, writing in place, the batched copy
-left running until the next step).  Every
-picture must still be bit-exact to the oracle."""
+"""The engine's pipelined use: steps issued back to back on its streams, the
+host reading step k-1 while step k runs, streams ending and new sessions
+taking their place without a drain, and the ways of queueing pictures (one
+host copy per call, the batched copy, writing in place, the batched copy
+left running until the next step, device pictures one call per session or
+in one batched call).  Every picture must still be bit-exact to the
+oracle."""
 import numpy as np
 import pytest
 
@@ -39,6 +40,9 @@ def _check(e, inst, where):
     return r.mbs
 
 
+_DEVICE_PICTURES = []
+
+
 def _queue(e, live, mode):
     sids = [i.sid for i in live]
     frames = [i.clip[i.pos] for i in live]
@@ -49,6 +53,18 @@ def _queue(e, live, mode):
         e.submit_frames(sids, frames)
     elif mode == 3:
         e.submit_frames(sids, frames, wait=False)   # copies finish inside the next step()
+    elif mode in (4, 5):
+        # pictures already in device memory, kept until the test ends
+        import torch
+        dev = [torch.from_numpy(np.ascontiguousarray(f)).to("cuda") for f in frames]
+        _DEVICE_PICTURES.extend(dev)
+        planes = [(d.data_ptr(), d.data_ptr() + i.w * i.h, d.data_ptr() + i.w * i.h * 5 // 4)
+                  for d, i in zip(dev, live)]
+        if mode == 4:
+            e.submit_device_batch(sids, *(np.array(c, np.uint64) for c in zip(*planes)))
+        else:
+            for s, p in zip(sids, planes):
+                e.submit_device(s, *p)
     else:
         arena, offs = e.inputs(sids)
         for inst, f, o in zip(live, frames, offs):
@@ -81,7 +97,7 @@ def test_pipelined_steps_with_turnover_match_oracle(gpu):
         prev, closing, step = None, [], 0
         while live or prev:
             if live:
-                _queue(e, live, step % 4)
+                _queue(e, live, step % 6)
                 assert e.step() == len(live)
             cur = list(live)
             # streams whose last picture is now queued make room for the next
@@ -135,6 +151,38 @@ def test_inputs_are_all_or_nothing(gpu):
         e.submit_frames([c], [fr])
         assert e.step() == 3
         e.sync()
+
+
+def test_device_batch_is_all_or_nothing(gpu):
+    import torch
+    with Engine(warps_per_cta=4) as e:
+        a = e.open(176, 144, 8)
+        b = e.open(176, 144, 8)
+        fr = synth.clip(0, 176, 144, 3, 1)[0]
+        d = torch.from_numpy(np.ascontiguousarray(fr)).to("cuda")
+        y = d.data_ptr()
+        cb, cr = y + 176 * 144, y + 176 * 144 * 5 // 4
+
+        def planes(*yy):
+            return [np.array(v, np.uint64) for v in (yy, [cb] * len(yy), [cr] * len(yy))]
+
+        with pytest.raises(RuntimeError):
+            e.submit_device_batch([a, a], *planes(y, y))        # a session twice
+        with pytest.raises(RuntimeError):
+            e.submit_device_batch([a, b], *planes(y, y + 8))    # Y not 16-byte aligned
+        with pytest.raises(RuntimeError):
+            e.submit_device_batch([a, 99], *planes(y, y))       # not open
+        e.submit_device(b, y, cb, cr)
+        with pytest.raises(RuntimeError):
+            e.submit_device_batch([a, b], *planes(y, y))        # b already queued
+        e.submit_device_batch([a], *planes(y))                  # nothing of the above stayed queued
+        assert e.step() == 2
+        e.sync()
+        ra, rb = e.result(a).to_abi(176), e.result(b).to_abi(176)
+        want = O.encode_sequence(fr[None], 176, 144, 8)["mbs"][0]
+        for got in (ra, rb):
+            for f in ("type", "flags", "quant", "cbp", "tcoeff"):
+                assert np.array_equal(got[f], want[f]), f
 
 
 def test_step_records_before_any_step(gpu):
