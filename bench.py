@@ -4,20 +4,23 @@
 One step = one frame-step of the workload: the next picture of every stream
 of the batch, encoded in one launch of the core (motion search, mode
 decision, motion compensation with the loop filter, DCT, denoise,
-quantisation, dequantisation, IDCT, reconstruction) followed by one launch
-of the bitstream writer (every picture's H.261 bytes).  Workload:
+quantisation, dequantisation, IDCT, reconstruction) followed by the three
+launches of the bitstream writer (every picture's H.261 bytes).  Workload:
 ``batch64`` (40 QCIF + 24 CIF streams, QUANT 4..24, lengths 30..300,
 seeded synthetic content; see h261enc_cuda_b200/workloads.py).
 
   value   device throughput: pictures already in HBM, L2 flushed (256 MiB
-          write) before every timed step, both kernels timed with CUDA
-          events on the engine's stream;
+          write) before every timed step, the encode and bitstream kernels
+          timed with CUDA events on the engine's stream;
   e2e     the same through the public API with host buffers: every step
           copies the pictures of all streams from host memory into the
-          pinned staging arena (h261b_engine_submit_batch, the engine's copy
-          threads), moves them to the device, encodes, writes the
-          bitstreams into mapped host memory and copies the MB records
-          back; the host moves step k-1's bitstreams out while step k runs;
+          pinned staging arena (h261b_engine_submit_batch_async, the
+          engine's copy threads), moves them to the device, encodes, writes
+          the bitstreams into mapped host memory and copies the MB records
+          back; the host moves step k-2's bitstreams out while steps k-1
+          and k run;
+  pipelined_device  pictures in HBM, steps back to back, three in flight:
+          the device's own pace;
   single_stream  the same streams one at a time (one picture per step,
           synchronous), the plain single-stream path;
   latency_ms     per-picture latency: batched = submit of a step -> its
@@ -359,7 +362,7 @@ def ours(args, world, rank, local, dist):
     eng = Engine(device=local, max_sessions=4 * len(streams), levels_to_host=0, me_mode=me_mode)
     run = Runner(eng, streams, pools)
     # warm-up (includes the launch-shape tuning steps), both input paths on
-    # both step parities
+    # every step slot
     for i in range(max(args.warmup, 8)):
         run.queue_device() if (i // 2) % 2 else run.queue_host()
         eng.step()
@@ -372,8 +375,8 @@ def ours(args, world, rank, local, dist):
     gc.collect()
     gc.disable()
 
-    # ---- value: device-resident pictures, L2 flushed, the step's two
-    # kernels (encode, bitstream) timed with CUDA events on its stream
+    # ---- value: device-resident pictures, L2 flushed, the step's encode
+    # kernel and its bitstream kernels timed with CUDA events on its stream
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
