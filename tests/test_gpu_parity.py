@@ -27,10 +27,10 @@ def assert_mbs_equal(got, want, where):
     assert bad.size == 0, f"{where}: levels differ at MBs {bad[:8].tolist()}"
 
 
-def run_engine(frames, w, h, quant, intra=0, me_mode=0, warps=4, fmad=1):
+def run_engine(frames, w, h, quant, intra=0, me_mode=0, warps=4, fmad=1, denoise=5):
     out_mbs, out_rec = [], []
     with Engine(me_mode=me_mode, warps_per_cta=warps, fmad=fmad) as e:
-        sid = e.open(w, h, quant, intra_period=intra)
+        sid = e.open(w, h, quant, intra_period=intra, denoise=denoise)
         for i in range(frames.shape[0]):
             e.submit_frame(sid, frames[i])
             assert e.step() == 1
@@ -57,6 +57,39 @@ def test_engine_matches_oracle(gpu, preset, w, h, n, quant, intra, me_mode):
     for i in range(n):
         assert_mbs_equal(got_mbs[i], want["mbs"][i], f"frame {i}")
         assert np.array_equal(got_rec[i], want["recon"][i]), f"frame {i}: reconstruction differs"
+
+
+@pytest.mark.parametrize("w,h,denoise", [
+    (176, 144, 0),     # no denoise: the offsets stay zero
+    (176, 144, 1),
+    (352, 288, 12),    # strong denoise: large offsets, more levels shrunk to zero
+])
+def test_denoise_strength_matches_oracle(gpu, w, h, denoise):
+    """The denoise strength scales the per-position offsets the frame end
+    computes from the noise statistics (mbgpu_kernels.cuh:478-503); the
+    default 5 is what the golden fixtures pin, the others must follow the
+    same arithmetic."""
+    n = 6
+    fr = synth.clip(2, w, h, 40 + denoise, n)
+    want = O.encode_sequence(fr, w, h, 6, intra_period=4, denoise=denoise)
+    got_mbs, got_rec = run_engine(fr, w, h, 6, intra=4, denoise=denoise)
+    for i in range(n):
+        assert_mbs_equal(got_mbs[i], want["mbs"][i], f"denoise {denoise} frame {i}")
+        assert np.array_equal(got_rec[i], want["recon"][i]), f"denoise {denoise} frame {i}: reconstruction differs"
+
+
+def test_unfused_arithmetic_matches_oracle(gpu):
+    """fmad=0 (step_kernel<0>) reproduces the reference built with
+    -fmad=false: every product rounded on its own.  Intra-heavy CIF content
+    at a fine quantiser, where the fused and unfused IDCTs part in rare
+    blocks."""
+    n = 4
+    fr = synth.clip(1, 352, 288, 77, n)
+    want = O.encode_sequence(fr, 352, 288, 2, intra_period=2, fmad=0)
+    got_mbs, got_rec = run_engine(fr, 352, 288, 2, intra=2, fmad=0)
+    for i in range(n):
+        assert_mbs_equal(got_mbs[i], want["mbs"][i], f"fmad=0 frame {i}")
+        assert np.array_equal(got_rec[i], want["recon"][i]), f"fmad=0 frame {i}: reconstruction differs"
 
 
 @pytest.mark.parametrize("warps", [1, 2, 8])
