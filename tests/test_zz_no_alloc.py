@@ -60,15 +60,16 @@ class DevPicture:
                                a[self.off_cr:self.off_cr + self.nc]])
 
 
-def test_noalloc_matches_engine_on_two_calls(gpu):
+@pytest.mark.parametrize("w,h,me_mode,fmad", [(176, 144, 0, 1), (352, 288, 1, 0)])
+def test_noalloc_matches_engine_on_two_calls(gpu, w, h, me_mode, fmad):
     import torch
     lib = _lib_noalloc()
-    w, h, q = 176, 144, 8
+    q = 8
     nmb = (w // 16) * (h // 16)
     frames = synth.clip(0, w, h, 41, 2)
 
     want = []
-    with Engine(warps_per_cta=4) as e:
+    with Engine(warps_per_cta=4, me_mode=me_mode, fmad=fmad) as e:
         sid = e.open(w, h, q)
         for i in range(2):
             e.submit_frame(sid, frames[i])
@@ -86,7 +87,7 @@ def test_noalloc_matches_engine_on_two_calls(gpu):
     stream = torch.cuda.current_stream().cuda_stream
     for i in range(2):
         p = NoallocPicture()
-        p.width, p.height, p.quant, p.me_mode, p.fmad, p.denoise = w, h, q, 0, 1, 5
+        p.width, p.height, p.quant, p.me_mode, p.fmad, p.denoise = w, h, q, me_mode, fmad, 5
         p.frame_type = 0 if i == 0 else 1
         p.reset_state = 1 if i == 0 else 0
         p.cur_y, p.cur_cb, p.cur_cr = cur[i].planes()
