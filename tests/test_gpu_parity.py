@@ -185,3 +185,37 @@ def test_reference_host_code_on_our_core(gpu, w, h, n, quant, intra, preset):
             assert a["quant"] == c["quant"] and a["bytes"] == c["bytes"]
             assert np.array_equal(a["me"], c["me"]) and np.array_equal(a["md"], c["md"])
             assert np.array_equal(a["mbs"], c["mbs"])
+
+
+needs_ref_cuda = pytest.mark.skipif(
+    not all(os.path.exists(O.DRIVERS[k]) for k in ("refgpu", "refgpu_nofmad", "ours")),
+    reason="the reference CUDA drivers are not built")
+
+
+@needs_ref_cuda
+@pytest.mark.parametrize("ref,fmad,w,h,n,quant,intra,preset,seed", [
+    ("refgpu", "1", 176, 144, 10, 8, 0, 3, 501),          # per-block random motion, fixed QUANT
+    ("refgpu", "1", 352, 288, 5, 0, 132, 2, 502),         # CIF, CBR 384 kbit/s
+    ("refgpu_nofmad", "0", 352, 288, 4, 3, 2, 1, 503),    # -fmad=false build, intra every 2 pictures
+])
+def test_reference_cuda_live_matches_our_core(gpu, ref, fmad, w, h, n, quant, intra, preset, seed):
+    """The reference's own CUDA (src/gpu_device.cu with its ME and MB
+    kernels, built for sm_100a) and this core behind the same gpu_device.h
+    boundary, each driven by the same frame loop on the same fresh seeded
+    clip on this GPU: the same bitstream, reconstruction and boundary
+    values (vectors, costs, mode decisions, levels)."""
+    fr = synth.clip(preset, w, h, seed, n)
+    with tempfile.TemporaryDirectory() as td:
+        yuv = os.path.join(td, "in.yuv")
+        fr.tofile(yuv)
+        rb, rrc, rd = O.run_driver(ref, yuv, w, h, n, td, quant=quant, intra=intra)
+        gb, grc, gd = O.run_driver("ours", yuv, w, h, n, td, quant=quant, intra=intra, env={"H261B_FMAD": fmad})
+        assert open(gb, "rb").read() == open(rb, "rb").read(), "bitstreams differ"
+        assert open(grc, "rb").read() == open(rrc, "rb").read(), "reconstructions differ"
+        frames = list(zip(O.read_dump(gd), O.read_dump(rd)))
+        assert len(frames) == n
+        for i, (a, c) in enumerate(frames):
+            assert a["quant"] == c["quant"] and a["bytes"] == c["bytes"], f"picture {i}"
+            assert np.array_equal(a["me"], c["me"]), f"picture {i}: ME results differ"
+            assert np.array_equal(a["md"], c["md"]), f"picture {i}: mode decisions differ"
+            assert np.array_equal(a["mbs"], c["mbs"]), f"picture {i}: macroblocks differ"
