@@ -4,8 +4,9 @@
  * staging arena by a small persistent pool: every plane copy is cut into
  * pieces of at most kPiece bytes, the pieces are taken from one atomic
  * counter by the workers and by the calling thread, and the call returns
- * when the last piece is done.  Workers sleep on a condition variable
- * between batches. */
+ * when the last piece is done.  A batch started without waiting is
+ * finished by the workers and by whichever thread joins it (the next
+ * step).  Workers sleep on a condition variable between batches. */
 #pragma once
 
 #include <atomic>
@@ -125,9 +126,12 @@ class CopyPool {
         publish(jobs);
     }
 
-    /* wait until the batch in flight (if any) is copied */
+    /* wait until the batch in flight (if any) is copied; the caller takes
+     * pieces of it meanwhile instead of only waiting */
     void join()
     {
+        if (left_.load(std::memory_order_acquire) != 0)
+            work();
         std::unique_lock<std::mutex> lk(m_);
         done_cv_.wait(lk, [this] { return left_.load(std::memory_order_acquire) == 0; });
     }
