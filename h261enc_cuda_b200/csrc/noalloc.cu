@@ -29,6 +29,7 @@
  */
 #include <cuda_runtime.h>
 
+#include <cstddef>
 #include <cstring>
 #include <mutex>
 
@@ -43,6 +44,7 @@ constexpr size_t kDescBytes = (sizeof(h261b_session_dev_t) + 255) / 256 * 256;
 constexpr size_t kScratchWords = kDescBytes / 4 + H261B_NOALLOC_MAX_MB;
 static_assert(sizeof(h261b_denoise_dev_t) == H261B_NOALLOC_STATE_BYTES, "state size");
 static_assert(sizeof(h261b_mb_info_t) == sizeof(h261b_mb_result_t), "result record size");
+static_assert(offsetof(h261b_denoise_dev_t, denoise) == 0, "the strength is the state's first word");
 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kScratchWords];
 
@@ -75,6 +77,22 @@ int scratch_for_device(int dev, uint32_t **out)
     }
     *out = g_addr[dev];
     return H261B_OK;
+}
+
+/* Writes the call's descriptor into the scratch and, for the first picture
+ * of a stream, clears the caller's denoise state and sets its strength (the
+ * reference's starting state, gpu_device.cu:495-508): offsets,
+ * accumulators and frame-end ticket zero. */
+__global__ void noalloc_prepare(h261b_session_dev_t d, h261b_session_dev_t *slot, uint32_t *state, int32_t reset,
+                                int32_t strength)
+{
+    if (reset) {
+        /* word 0 of h261b_denoise_dev_t is the strength */
+        for (int i = threadIdx.x; i < H261B_NOALLOC_STATE_BYTES / 4; i += blockDim.x)
+            state[i] = i == 0 ? (uint32_t)strength : 0u;
+    }
+    if (threadIdx.x == 0)
+        *slot = d;
 }
 
 } // namespace
@@ -125,14 +143,6 @@ extern "C" int h261b_encode_picture_noalloc(const h261b_noalloc_picture_t *p, vo
         return rc;
     cudaStream_t st = (cudaStream_t)stream;
 
-    if (p->reset_state) {
-        /* a new stream: zero offsets, accumulators and ticket, then the
-         * strength (the reference's starting state, gpu_device.cu:495-508) */
-        H261B_CUDA_TRY(cudaMemsetAsync(p->state, 0, H261B_NOALLOC_STATE_BYTES, st));
-        const int32_t strength = p->denoise;
-        H261B_CUDA_TRY(cudaMemcpyAsync(p->state, &strength, sizeof(strength), cudaMemcpyHostToDevice, st));
-    }
-
     h261b_session_dev_t d;
     memset(&d, 0, sizeof(d));
     d.cur_y = p->cur_y;
@@ -155,7 +165,12 @@ extern "C" int h261b_encode_picture_noalloc(const h261b_noalloc_picture_t *p, vo
     d.dn = (h261b_denoise_dev_t *)p->state;
     d.info_out = (h261b_mb_info_t *)p->mbs;
     d.level_out = p->levels;
-    H261B_CUDA_TRY(cudaMemcpyAsync(scratch, &d, sizeof(d), cudaMemcpyHostToDevice, st));
+    /* the descriptor (and, for a new stream, the cleared state with its
+     * strength) goes to the device as kernel arguments: no host buffer has
+     * to outlive the call */
+    noalloc_prepare<<<1, 256, 0, st>>>(d, (h261b_session_dev_t *)scratch, (uint32_t *)p->state,
+                                       p->reset_state ? 1 : 0, p->denoise);
+    H261B_CUDA_TRY(cudaGetLastError());
     const int phases = H261B_PHASE_ME | H261B_PHASE_MD | H261B_PHASE_ENCDEC | (p->fmad ? 0x100 : 0);
     const int lr = h261b_launch_step((const h261b_session_dev_t *)scratch,
                                      (const uint32_t *)((const uint8_t *)scratch + kDescBytes), nmb, phases, 4, 0,

@@ -126,6 +126,21 @@ int32_t orc_rc_picture_quant(orc_rc_t *rc, int32_t frame_type, int32_t picture_c
 /* after the picture: its QUANT and its size in bytes */
 void orc_rc_update(orc_rc_t *rc, int32_t frame_type, int32_t quant, int32_t bytes);
 
+/* one encode stream of the reference's frame loop (h261_main.c:173-271
+ * plus an intra period), a picture at a time: fixed QUANT when quant > 0,
+ * else CBR rate control started at QUANT 10 with VBV = bitrate.  The state
+ * between pictures is the reference picture, denoise offsets, rate control
+ * and picture counter.  orc_stream_encode writes one picture's bytes to out
+ * and returns their count (-1: out_cap too small, other negatives as
+ * orc_write_picture); quant_out and recon_out optional.  Streams are
+ * independent: different streams may be encoded on different threads. */
+typedef struct orc_stream orc_stream_t;
+orc_stream_t *orc_stream_open(int32_t w, int32_t h, int32_t quant, int32_t bitrate, int32_t intra_period,
+                              int32_t denoise, int32_t fmad, int32_t me_mode);
+int32_t orc_stream_encode(orc_stream_t *s, const uint8_t *picture, uint8_t *out, int32_t out_cap,
+                          int32_t *quant_out, uint8_t *recon_out);
+void orc_stream_close(orc_stream_t *s);
+
 /* the reference encoder's whole frame loop (h261_main.c:178-275 plus an
  * intra period): fixed QUANT when quant > 0, else CBR rate control started
  * at QUANT 10 with VBV = bitrate.  Writes the concatenated pictures to bits

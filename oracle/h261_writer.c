@@ -399,71 +399,138 @@ void orc_rc_update(orc_rc_t *rc, int32_t frame_type, int32_t quant, int32_t byte
 
 /* ------------------------------------------------------------ the stream */
 
+/* one stream's state between pictures: the reference picture, denoise
+ * offsets, rate control and picture counter (what h261_main.c keeps across
+ * its frame loop, :173-271) */
+struct orc_stream {
+    int32_t w, h, nmb, quant, bitrate, intra_period, fmad, me_mode, frame;
+    size_t fs, ny, nc;
+    uint8_t *ref, *rec, *pic;
+    me_gpu_mb_t *me;
+    h261_mb_mode_decision_t *md;
+    h261_macroblock_t *mbs;
+    h261_dct_denoise_t dn;
+    orc_rc_t rc;
+};
+
+/* one picture is at most 32 + 12 * 26 + 396 * 7749 bits */
+#define ORC_PIC_CAP (400 * 1024)
+
+orc_stream_t *orc_stream_open(int32_t w, int32_t h, int32_t quant, int32_t bitrate, int32_t intra_period,
+                              int32_t denoise, int32_t fmad, int32_t me_mode)
+{
+    if (!((w == 176 && h == 144) || (w == 352 && h == 288)) || quant > 31)
+        return NULL;
+    orc_stream_t *s = (orc_stream_t *)calloc(1, sizeof(orc_stream_t));
+    if (!s)
+        return NULL;
+    s->w = w;
+    s->h = h;
+    s->nmb = (w / 16) * (h / 16);
+    s->quant = quant;
+    s->bitrate = bitrate;
+    s->intra_period = intra_period;
+    s->fmad = fmad;
+    s->me_mode = me_mode;
+    s->fs = (size_t)w * h * 3 / 2;
+    s->ny = (size_t)w * h;
+    s->nc = s->ny / 4;
+    s->ref = (uint8_t *)calloc(s->fs, 1);   /* the first reference is black */
+    s->rec = (uint8_t *)calloc(s->fs, 1);
+    s->pic = (uint8_t *)malloc(ORC_PIC_CAP);
+    s->me = (me_gpu_mb_t *)calloc((size_t)s->nmb, sizeof(me_gpu_mb_t));
+    s->md = (h261_mb_mode_decision_t *)calloc((size_t)s->nmb, sizeof(h261_mb_mode_decision_t));
+    s->mbs = (h261_macroblock_t *)calloc((size_t)s->nmb, sizeof(h261_macroblock_t));
+    if (!s->ref || !s->rec || !s->pic || !s->me || !s->md || !s->mbs) {
+        orc_stream_close(s);
+        return NULL;
+    }
+    orc_denoise_init(&s->dn, denoise);
+    orc_rc_init(&s->rc, 10, bitrate, bitrate);
+    for (int32_t i = 0; i < s->nmb; i++) {
+        s->mbs[i].i_mb_x = (i % (w / 16)) * 16;
+        s->mbs[i].i_mb_y = (i / (w / 16)) * 16;
+    }
+    return s;
+}
+
+void orc_stream_close(orc_stream_t *s)
+{
+    if (!s)
+        return;
+    free(s->ref);
+    free(s->rec);
+    free(s->pic);
+    free(s->me);
+    free(s->md);
+    free(s->mbs);
+    free(s);
+}
+
+int32_t orc_stream_encode(orc_stream_t *s, const uint8_t *cur, uint8_t *out, int32_t out_cap, int32_t *quant_out,
+                          uint8_t *recon_out)
+{
+    const int32_t w = s->w, h = s->h, nmb = s->nmb, f = s->frame;
+    orc_me_frame(cur, s->ref, w, h, s->me_mode, s->me, NULL);
+    const int32_t ft = (f == 0 || (s->intra_period > 0 && f % s->intra_period == 0)) ? H261B_FRAME_TYPE_INTRA
+                                                                                   : H261B_FRAME_TYPE_INTER;
+    orc_mode_decision(s->me, nmb, ft, s->md);
+    int32_t q = s->quant;
+    if (s->quant <= 0) {
+        int32_t cost = 0;
+        for (int32_t i = 0; i < nmb; i++)
+            cost += s->md[i].i_cost;
+        q = orc_rc_picture_quant(&s->rc, ft, cost, nmb);
+    }
+    orc_frame_t c = { cur, cur + s->ny, cur + s->ny + s->nc }, r = { s->ref, s->ref + s->ny, s->ref + s->ny + s->nc };
+    orc_encode_frame(&c, &r, w, h, s->md, q, &s->dn, s->fmad, s->mbs);
+    const int32_t nb = orc_write_picture(w, h, f, ft, q, s->mbs, s->pic, ORC_PIC_CAP);
+    if (nb < 0)
+        return nb;
+    if (nb > out_cap)
+        return -1;
+    memcpy(out, s->pic, (size_t)nb);
+    if (quant_out)
+        *quant_out = q;
+    if (s->quant <= 0)
+        orc_rc_update(&s->rc, ft, q, nb);
+    orc_frame_out_t o = { s->rec, s->rec + s->ny, s->rec + s->ny + s->nc };
+    orc_decode_frame(&r, w, h, s->mbs, s->fmad, &o);
+    uint8_t *t = s->ref;
+    s->ref = s->rec;
+    s->rec = t;
+    if (recon_out)
+        memcpy(recon_out, s->ref, s->fs);
+    s->frame++;
+    return nb;
+}
+
 int64_t orc_encode_stream(const uint8_t *yuv, int32_t w, int32_t h, int32_t nframes, int32_t quant,
                           int32_t bitrate, int32_t intra_period, int32_t denoise, int32_t fmad,
                           int32_t me_mode, uint8_t *bits, int64_t bits_cap, int32_t *frame_bytes,
                           int32_t *frame_quant, uint8_t *recon_out)
 {
-    if (!((w == 176 && h == 144) || (w == 352 && h == 288)) || quant > 31)
+    orc_stream_t *s = orc_stream_open(w, h, quant, bitrate, intra_period, denoise, fmad, me_mode);
+    if (!s)
         return -2;
-    const int32_t nmb = (w / 16) * (h / 16);
-    const size_t fs = (size_t)w * h * 3 / 2, ny = (size_t)w * h, nc = ny / 4;
-    /* one picture is at most 32 + 12 * 26 + 396 * 7749 bits */
-    const int32_t pic_cap = 400 * 1024;
-    uint8_t *ref = (uint8_t *)calloc(fs, 1), *rec = (uint8_t *)calloc(fs, 1);
-    uint8_t *pic = (uint8_t *)malloc(pic_cap);
-    me_gpu_mb_t *me = (me_gpu_mb_t *)calloc((size_t)nmb, sizeof(me_gpu_mb_t));
-    h261_mb_mode_decision_t *md = (h261_mb_mode_decision_t *)calloc((size_t)nmb, sizeof(*md));
-    h261_macroblock_t *mbs = (h261_macroblock_t *)calloc((size_t)nmb, sizeof(h261_macroblock_t));
-    h261_dct_denoise_t dn;
-    orc_rc_t rc;
-    orc_denoise_init(&dn, denoise);
-    orc_rc_init(&rc, 10, bitrate, bitrate);
-    for (int32_t i = 0; i < nmb; i++) {
-        mbs[i].i_mb_x = (i % (w / 16)) * 16;
-        mbs[i].i_mb_y = (i / (w / 16)) * 16;
-    }
     int64_t total = 0;
-    for (int32_t f = 0; f < nframes && total >= 0; f++) {
-        const uint8_t *cur = yuv + (size_t)f * fs;
-        orc_me_frame(cur, ref, w, h, me_mode, me, NULL);
-        const int32_t ft = (f == 0 || (intra_period > 0 && f % intra_period == 0)) ? H261B_FRAME_TYPE_INTRA
-                                                                                 : H261B_FRAME_TYPE_INTER;
-        orc_mode_decision(me, nmb, ft, md);
-        int32_t q = quant;
-        if (quant <= 0) {
-            int32_t cost = 0;
-            for (int32_t i = 0; i < nmb; i++)
-                cost += md[i].i_cost;
-            q = orc_rc_picture_quant(&rc, ft, cost, nmb);
-        }
-        orc_frame_t c = { cur, cur + ny, cur + ny + nc }, r = { ref, ref + ny, ref + ny + nc };
-        orc_encode_frame(&c, &r, w, h, md, q, &dn, fmad, mbs);
-        const int32_t nb = orc_write_picture(w, h, f, ft, q, mbs, pic, pic_cap);
-        if (nb < 0 || total + nb > bits_cap) {
-            total = nb < 0 ? nb : -1;
+    for (int32_t f = 0; f < nframes; f++) {
+        const int64_t room = bits_cap - total;
+        int32_t q = 0;
+        const int32_t nb = orc_stream_encode(s, yuv + (size_t)f * s->fs, bits + total,
+                                             room > ORC_PIC_CAP ? ORC_PIC_CAP : (int32_t)room, &q,
+                                             recon_out ? recon_out + (size_t)f * s->fs : NULL);
+        if (nb < 0) {
+            total = nb;
             break;
         }
-        memcpy(bits + total, pic, (size_t)nb);
         total += nb;
         if (frame_bytes)
             frame_bytes[f] = nb;
         if (frame_quant)
             frame_quant[f] = q;
-        if (quant <= 0)
-            orc_rc_update(&rc, ft, q, nb);
-        orc_frame_out_t o = { rec, rec + ny, rec + ny + nc };
-        orc_decode_frame(&r, w, h, mbs, fmad, &o);
-        memcpy(ref, rec, fs);
-        if (recon_out)
-            memcpy(recon_out + (size_t)f * fs, rec, fs);
     }
-    free(ref);
-    free(rec);
-    free(pic);
-    free(me);
-    free(md);
-    free(mbs);
+    orc_stream_close(s);
     return total;
 }
 

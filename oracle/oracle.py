@@ -70,6 +70,11 @@ def lib() -> ctypes.CDLL:
         L.orc_encode_stream.argtypes = [c_void_p] + [c_int32] * 9 + [c_void_p, ctypes.c_int64, c_void_p,
                                                                         c_void_p, c_void_p]
         L.orc_encode_stream.restype = ctypes.c_int64
+        L.orc_stream_open.argtypes = [c_int32] * 8
+        L.orc_stream_open.restype = c_void_p
+        L.orc_stream_encode.argtypes = [c_void_p, c_void_p, c_void_p, c_int32, POINTER(c_int32), c_void_p]
+        L.orc_stream_encode.restype = c_int32
+        L.orc_stream_close.argtypes = [c_void_p]
         L.orc_decode_stream.argtypes = [c_void_p, ctypes.c_int64, c_int32, c_void_p, c_int32, c_void_p,
                                         POINTER(c_int32), POINTER(c_int32), POINTER(c_int32)]
         L.orc_decode_stream.restype = ctypes.c_int64
@@ -162,6 +167,46 @@ def encode_stream(frames: np.ndarray, width: int, height: int, quant: int = 0, b
     if total < 0:
         raise ValueError(f"orc_encode_stream: status {total}")
     return bits[:total].tobytes(), nb, nq, recon
+
+
+class Stream:
+    """One encode stream of the oracle's frame loop, a picture at a time
+    (orc_stream_*): ``encode(picture)`` returns the picture's H.261 bytes.
+    The C call releases the GIL, so streams encode in parallel on threads."""
+
+    def __init__(self, width: int, height: int, quant: int = 0, bitrate: int = 384000, intra_period: int = 0,
+                 denoise: int = 5, fmad: int = 1, me_mode: int = 0):
+        self._h = lib().orc_stream_open(width, height, quant, bitrate, intra_period, denoise, fmad, me_mode)
+        if not self._h:
+            raise ValueError(f"orc_stream_open: no stream of {width}x{height} QUANT {quant}")
+        self._out = np.empty(400 * 1024, np.uint8)
+        self.quant = 0
+
+    def encode(self, picture: np.ndarray) -> bytes:
+        n = self.encode_count(picture)
+        return self._out[:n].tobytes()
+
+    def encode_count(self, picture: np.ndarray) -> int:
+        """Encode and return the byte count only (the bytes stay in an
+        internal buffer until the next call)."""
+        q = c_int32()
+        n = lib().orc_stream_encode(self._h, _p(np.ascontiguousarray(picture, np.uint8)), _p(self._out),
+                                    self._out.size, ctypes.byref(q), None)
+        if n < 0:
+            raise ValueError(f"orc_stream_encode: status {n}")
+        self.quant = q.value
+        return n
+
+    def close(self) -> None:
+        if self._h:
+            lib().orc_stream_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def decode_stream(bits: bytes, max_frames: int = 1024, fmad: int = 1):

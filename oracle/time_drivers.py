@@ -32,35 +32,36 @@ CASES = [
 ]
 
 
+def time_driver(kind: str, preset: int, w: int, h: int, q: int, seed: int, frames: int, tmp: str):
+    """Encode one seeded clip with one driver, timing every picture: per
+    picture ms (the first left out), MB/s and the bitstream's SHA-256."""
+    clip = synth.clip(preset, w, h, seed, frames)
+    d = os.path.join(tmp, f"{kind}_{w}x{h}_{q}_{seed}_{frames}")
+    os.makedirs(d, exist_ok=True)
+    yuv = os.path.join(d, "in.yuv")
+    clip.tofile(yuv)
+    timing = os.path.join(d, "timing.txt")
+    bits = os.path.join(d, "out.h261")
+    args = [O.DRIVERS[kind], f"in={yuv}", f"w={w}", f"h={h}", f"frames={frames}", f"bits={bits}",
+            f"recon={os.path.join(d, 'recon.yuv')}", f"dump={os.path.join(d, 'dump.bin')}",
+            f"timing={timing}", "intra=132" if q == 0 else "intra=0",
+            f"quant={q}" if q > 0 else "bitrate=384000"]
+    subprocess.run(args, check=True, stdout=subprocess.DEVNULL, timeout=600)
+    ms = [float(x) for x in open(timing).read().split()]
+    steady = ms[1:]
+    nmb = (w // 16) * (h // 16)
+    return {"ms_per_picture_median": statistics.median(steady), "ms_per_picture_mean": statistics.mean(steady),
+            "ms_per_picture_p99": sorted(steady)[min(len(steady) - 1, int(0.99 * len(steady)))],
+            "mb_per_s": nmb * len(steady) / (sum(steady) * 1e-3), "pictures": len(steady),
+            "sha256": hashlib.sha256(open(bits, "rb").read()).hexdigest()}
+
+
 def run(frames: int):
     out = {}
     with tempfile.TemporaryDirectory() as tmp:
         for name, preset, w, h, q, seed in CASES:
-            clip = synth.clip(preset, w, h, seed, frames)
-            yuv = os.path.join(tmp, f"{name}.yuv")
-            clip.tofile(yuv)
-            row = {}
-            digests = {}
-            for kind in ("refgpu", "ours"):
-                d = os.path.join(tmp, f"{name}_{kind}")
-                os.makedirs(d)
-                exe = O.DRIVERS[kind]
-                timing = os.path.join(d, "timing.txt")
-                bits = os.path.join(d, "out.h261")
-                args = [exe, f"in={yuv}", f"w={w}", f"h={h}", f"frames={frames}", f"bits={bits}",
-                        f"recon={os.path.join(d, 'recon.yuv')}", f"dump={os.path.join(d, 'dump.bin')}",
-                        f"timing={timing}", "intra=132" if q == 0 else "intra=0",
-                        f"quant={q}" if q > 0 else "bitrate=384000"]
-                subprocess.run(args, check=True, stdout=subprocess.DEVNULL, timeout=600)
-                ms = [float(x) for x in open(timing).read().split()]
-                digests[kind] = hashlib.sha256(open(bits, "rb").read()).hexdigest()
-                steady = ms[1:]
-                nmb = (w // 16) * (h // 16)
-                row[kind] = {"ms_per_picture_median": statistics.median(steady),
-                             "ms_per_picture_mean": statistics.mean(steady),
-                             "mb_per_s": nmb * len(steady) / (sum(steady) * 1e-3),
-                             "pictures": len(steady)}
-            row["same_bitstream"] = digests["refgpu"] == digests["ours"]
+            row = {kind: time_driver(kind, preset, w, h, q, seed, frames, tmp) for kind in ("refgpu", "ours")}
+            row["same_bitstream"] = row["refgpu"].pop("sha256") == row["ours"].pop("sha256")
             row["speedup"] = row["ours"]["mb_per_s"] / row["refgpu"]["mb_per_s"]
             out[name] = row
     return out

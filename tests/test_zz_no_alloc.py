@@ -87,7 +87,10 @@ def test_noalloc_matches_engine_on_two_calls(gpu, w, h, me_mode, fmad):
     stream = torch.cuda.current_stream().cuda_stream
     for i in range(2):
         p = NoallocPicture()
-        p.width, p.height, p.quant, p.me_mode, p.fmad, p.denoise = w, h, q, me_mode, fmad, 5
+        # the strength is read on the first call only (reset_state): the
+        # second call's 9 must be ignored, as the engine's session keeps 5
+        p.width, p.height, p.quant, p.me_mode, p.fmad = w, h, q, me_mode, fmad
+        p.denoise = 5 if i == 0 else 9
         p.frame_type = 0 if i == 0 else 1
         p.reset_state = 1 if i == 0 else 0
         p.cur_y, p.cur_cb, p.cur_cr = cur[i].planes()
