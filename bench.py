@@ -64,6 +64,10 @@ ALG_BYTES_PER_MB = 384 + 384 + 384 + 384 + 16 + 4
 # reference-mode search: 121 + 49 candidates x 256 absolute differences
 SAD_PER_MB = 170 * 256
 SAD_PER_MB_FULL = 961 * 256
+# the plain single-stream configurations: name, synthetic preset, size,
+# QUANT (0: CBR 384 kbit/s with an intra picture every 132), seed, pictures
+PLAIN_CONFIGS = [("qcif_q8_30", 0, 176, 144, 8, 2026, 30),
+                 ("cif_cbr384k_300", 1, 352, 288, 0, 2027, 300)]
 
 
 def parse():
@@ -77,6 +81,10 @@ def parse():
                     help="motion search: the reference's grid + refinement (bit-exact), or every vector "
                          "of [-15,15]^2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="reference arm: skip timing the reference's own CUDA on the plain configurations")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the plain single-stream, stress1024 and serving legs of the batch64 line")
     ap.add_argument("--serve-seconds", type=float, default=20.0,
                     help="length of the serving run (--workload serve)")
     return ap.parse_args()
@@ -203,26 +211,111 @@ def dist_setup(args):
 
 # ------------------------------------------------------------ CPU baseline
 
-def cpu_baseline(streams, frames_per_stream: int, threads: int):
+# untimed steps before either arm's timed steps (at least the --warmup
+# given): they cover the engine's tuning of its launch plan, which runs on
+# its first mostly-inter steps (18 of them)
+WARM_STEPS = 24
+
+
+def workload_config(args, streams, mb_per_step, world):
+    """The config both arms report: the same streams, pictures and positions."""
+    me_full = getattr(args, "me", "reference") == "full"
+    return {"workload": args.workload, "streams": len(streams), "mb_per_step": mb_per_step,
+            "positions": f"steps {max(args.warmup, WARM_STEPS)}..{max(args.warmup, WARM_STEPS) + args.steps - 1} "
+                         f"of every stream's {CLIP_LEN}-picture forwards-backwards clip, restarts at each "
+                         "stream's length",
+            "me_mode": ("full (every vector of [-15,15]^2; not bit-exact to the reference)" if me_full
+                        else "reference (11x11 grid + 7x7 refinement)"),
+            "l2": "GPU arm: flushed before every timed step (256 MiB write)",
+            "parallelism": f"sessions x{world}"}
+
+
+class CpuRunner:
     """The oracle (C restatement of the reference's encoder: device path,
-    rate-control-free frame loop and bitstream writer) over a bounded
-    sample: each task encodes one stream's first pictures to H.261 bytes."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
+    frame loop and bitstream writer) fed exactly as ``Runner`` feeds the
+    engine: stream j plays its clip forwards and backwards from picture 0,
+    and a stream that reaches its length restarts as a new stream (intra
+    picture, black reference).  One step encodes the next picture of every
+    stream to H.261 bytes, the streams spread over a thread pool (the C
+    encoder releases the GIL), largest pictures first."""
+
+    def __init__(self, streams, clips, threads, clip_len=CLIP_LEN):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        from h261enc_cuda_b200 import workloads
+        self.O, self.streams, self.clips = O, streams, clips
+        self.enc = [None] * len(streams)
+        self.pos = [0] * len(streams)
+        self.period = max(2 * clip_len - 2, 1)
+        self.index = [workloads.clip_index(k, clip_len) for k in range(self.period)]
+        self.order = sorted(range(len(streams)), key=lambda j: -streams[j].num_mb)
+        self.ex = ThreadPoolExecutor(max_workers=threads)
+        O.lib()
+
+    def _one(self, j):
+        s = self.streams[j]
+        if self.enc[j] is None or self.pos[j] >= s.length:
+            if self.enc[j] is not None:
+                self.enc[j].close()
+            self.enc[j] = self.O.Stream(s.width, s.height, quant=s.quant)
+            self.pos[j] = 0
+        self.enc[j].encode_count(self.clips[j][self.index[self.pos[j] % self.period]])
+        self.pos[j] += 1
+        return s.num_mb
+
+    def step(self):
+        """(MBs, seconds) of one step."""
+        t = time.perf_counter()
+        mbs = sum(self.ex.map(self._one, self.order))
+        return mbs, time.perf_counter() - t
+
+    def close(self):
+        self.ex.shutdown()
+        for e in self.enc:
+            if e is not None:
+                e.close()
+
+
+def cpu_clips(streams):
     from h261enc_cuda_b200 import workloads
-    clips = [workloads.make_clip(s, frames_per_stream) for s in streams]
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        return list(ex.map(lambda s: workloads.make_clip(s, CLIP_LEN), streams))
 
-    def task(i):
-        s = streams[i]
-        O.encode_stream(clips[i], s.width, s.height, quant=s.quant)
-        return s.num_mb * frames_per_stream
 
-    O.lib()
-    t = time.perf_counter()
-    with ThreadPoolExecutor(max_workers=threads) as ex:
-        mbs = sum(ex.map(task, range(len(streams))))
-    el = time.perf_counter() - t
-    return mbs, el
+def cpu_steps(streams, clips, warm, steps, threads):
+    """Per-step (MBs, seconds) of the oracle over timed steps warm ..
+    warm + steps - 1 (the first `warm` steps run untimed)."""
+    run = CpuRunner(streams, clips, threads)
+    try:
+        for _ in range(warm):
+            run.step()
+        return [run.step() for _ in range(steps)]
+    finally:
+        run.close()
+
+
+def reference_cuda_single_stream():
+    """The reference's own CUDA (src/gpu_device.cu built for sm_100a,
+    oracle/_ref/h261_drive_refgpu) through its frame loop, one stream: the
+    plain single-stream configurations -- QCIF, 30 pictures, QUANT 8 (first
+    picture intra), and CIF, 300 pictures, CBR 384 kbit/s, intra every 132,
+    with a scene cut -- timed picture by picture by the driver."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import tempfile
+    import oracle as O
+    if not os.path.exists(O.DRIVERS["refgpu"]):
+        return {"unavailable": "oracle/_ref/h261_drive_refgpu is not built"}
+    import time_drivers as T
+    from h261enc_cuda_b200 import synth
+    out = {}
+    try:
+        with tempfile.TemporaryDirectory() as tmp:
+            for name, preset, w, h, q, seed, n in PLAIN_CONFIGS:
+                out[name] = T.time_driver("refgpu", preset, w, h, q, seed, n, tmp)
+                out[name].pop("sha256")
+    except Exception as exc:  # no GPU for the reference's CUDA on this host
+        return {"unavailable": f"{type(exc).__name__}: {str(exc)[:160]}"}
+    return out
 
 
 def reference_arm(args, world, rank):
@@ -235,22 +328,24 @@ def reference_arm(args, world, rank):
         return
     streams = workloads.WORKLOADS[args.workload]()
     threads = os.cpu_count() or 1
-    frames = 3
-    for _ in range(args.warmup):
-        cpu_baseline(streams[:threads], 2, threads)
-    times, total = [], 0
-    for _ in range(args.steps):
-        mbs, el = cpu_baseline(streams, frames, threads)
-        times.append(el)
-        total += mbs
-    value = total / sum(times)
-    sample = f"{len(streams)} streams x {frames} pictures to bitstreams per step (oracle, C, -O2)"
+    clips = cpu_clips(streams)
+    warm = max(args.warmup, WARM_STEPS)
+    per_step = cpu_steps(streams, clips, warm, args.steps, threads)
+    total = sum(m for m, _ in per_step)
+    secs = sum(t for _, t in per_step)
+    value = total / secs
+    mb_per_step = total // args.steps
+    sample = (f"the GPU arm's timed steps: {len(streams)} streams x {args.steps} steps ({mb_per_step} MBs per "
+              f"step) after {warm} untimed steps, to bitstreams (oracle, C, -O3, {threads} threads)")
     line = {"impl": "reference", "metric": METRICS[args.workload], "value": value, "unit": "MB/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-            "config": {"workload": args.workload, "streams": len(streams), "mb_per_step": total // args.steps},
-            "cpu_baseline": {"value": value, "unit": "MB/s", "cores": threads, "kind": "port", "sample": sample},
+            "config": workload_config(args, streams, mb_per_step, world),
+            "cpu_baseline": {"value": value, "unit": "MB/s", "cores": threads, "kind": "port", "sample": sample,
+                             "per_core": value / threads},
             "e2e": {"value": value, "unit": "MB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if args.workload == "batch64" and not args.no_reference_cuda:
+        line["reference_cuda_single_stream"] = reference_cuda_single_stream()
     print(json.dumps(line), flush=True)
 
 
@@ -287,7 +382,7 @@ class Runner:
     returns a closed session's device slot to its pool when the steps in
     flight that use it have completed, so nothing drains here."""
 
-    def __init__(self, engine, streams, pools):
+    def __init__(self, engine, streams, pools, clip_len=CLIP_LEN):
         self.e, self.streams, self.pools = engine, streams, pools
         from h261enc_cuda_b200 import workloads
         self.sids = np.array([engine.open(s.width, s.height, s.quant, bitstream=1) for s in streams], np.int32)
@@ -300,8 +395,8 @@ class Runner:
         self.fbytes = np.array([p[1].shape[1] for p in pools], np.uint64)
         self.ny = np.array([s.width * s.height for s in streams], np.uint64)
         # clip picture of every position of one forwards-backwards period
-        self.period = max(2 * CLIP_LEN - 2, 1)
-        self.index = np.array([workloads.clip_index(k, CLIP_LEN) for k in range(self.period)], np.uint64)
+        self.period = max(2 * clip_len - 2, 1)
+        self.index = np.array([workloads.clip_index(k, clip_len) for k in range(self.period)], np.uint64)
         # device pictures: plane addresses per (stream, clip picture)
         self.dev = [np.array([[pl[i][c] for i in range(len(pl))] for pl in (p[2] for p in pools)], np.uint64)
                     for c in range(3)]
@@ -371,7 +466,7 @@ def ours(args, world, rank, local, dist):
     run = Runner(eng, streams, pools)
     # warm-up (includes the launch-shape tuning steps), both input paths on
     # every step slot
-    for i in range(max(args.warmup, 8)):
+    for i in range(max(args.warmup, WARM_STEPS)):
         run.queue_device() if (i // 2) % 2 else run.queue_host()
         eng.step()
         eng.sync()
@@ -455,7 +550,7 @@ def ours(args, world, rank, local, dist):
 
     # untimed warm-up of this loop: the value loop's device-input steps left
     # other graphs on the slots, so the host-input signature is recaptured here
-    pipeline(2, max(args.warmup, 8))
+    pipeline(2, max(args.warmup, WARM_STEPS))
     h2d = d2h = 0
     # five times the value loop's steps (still well under a second): a
     # single host hiccup of a few milliseconds would otherwise weigh on a
@@ -472,28 +567,58 @@ def ours(args, world, rank, local, dist):
 
     # ---- the device's own pace with steps back to back: pictures already
     # in HBM, three steps in flight, the host waiting for step k-2 only (the
-    # ceiling the end-to-end loop reaches when the host keeps up)
+    # ceiling the end-to-end loop reaches when the host keeps up).  Its own
+    # warm-up, then five times the value loop's steps, so that filling and
+    # draining the pipeline weighs little; every step's device timeline
+    # (h261b_engine_step_timing) is read as it completes.
+    def back_to_back(steps, phases):
+        first = run.queued
+        for it in range(steps):
+            run.queue_device()
+            eng.step()
+            if it >= 2:
+                eng.wait_step(first + it - 2)
+                if phases is not None:
+                    phases.append(eng.step_timing())
+                run.retire(first + it - 2)
+        for k in range(max(0, steps - 2), steps):
+            eng.wait_step(first + k)
+            if phases is not None:
+                phases.append(eng.step_timing())
+            run.retire(first + k)
+
+    back_to_back(max(args.warmup, WARM_STEPS), None)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    first = run.queued
+    piped_steps = 5 * args.steps
+    phases = []
     t0 = time.perf_counter()
-    for it in range(args.steps):
-        run.queue_device()
-        eng.step()
-        if it >= 2:
-            eng.wait_step(first + it - 2)
-            run.retire(first + it - 2)
+    back_to_back(piped_steps, phases)
     torch.cuda.synchronize()
     piped_s = shard.max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
-    piped = mb_per_step * args.steps * world / piped_s
+    piped = mb_per_step * piped_steps * world / piped_s
+    phase_ms = {k: float(np.median([ph[k] for ph in phases])) for k in ("upload", "wait", "encode", "bitstream",
+                                                                          "total")}
     graph_caps, graph_reps = eng.graph_stats()
     eng.destroy()
 
-    # ---- single stream: the same streams one at a time, one picture per step
+    # ---- single stream: the same streams one at a time, one picture per
+    # step.  An untimed stream of each size first: the engine's first steps
+    # size its arenas and host bitstream buffers and capture graphs, which
+    # is set-up, not the steady pace of one stream.
     single_lat, single_mbs = [], 0
-    eng1 = Engine(device=local, max_sessions=8, warps_per_cta=4, levels_to_host=0, me_mode=me_mode)
+    eng1 = Engine(device=local, max_sessions=8, levels_to_host=0, me_mode=me_mode)
     per_stream = 3
+    for (w, h) in sizes:
+        eng1.reserve(w, h, 2, bitstream=1)
+        k = next(i for i, s in enumerate(streams) if (s.width, s.height) == (w, h))
+        sid = eng1.open(w, h, streams[k].quant, bitstream=1)
+        for i in range(2 * per_stream):
+            eng1.submit_frame(sid, pools[k][1][i % CLIP_LEN])
+            eng1.step()
+            eng1.sync()
+        eng1.close(sid)
     t0 = time.perf_counter()
     for k, s in enumerate(streams):
         sid = eng1.open(s.width, s.height, s.quant, bitstream=1)
@@ -511,6 +636,13 @@ def ours(args, world, rank, local, dist):
     single = single_mbs / single_s
     if gc_was_on:
         gc.enable()
+    del pools, run
+
+    extra = {}
+    if args.workload == "batch64" and not args.no_extra:
+        extra["plain_single_stream"] = plain_single_stream(local, me_mode)
+        extra["stress1024"] = stress_leg(args, local, flush)
+        extra["serving"] = serving_leg(local, rank, seconds=10.0)
 
     if rank != 0:
         if dist:
@@ -531,10 +663,7 @@ def ours(args, world, rank, local, dist):
         "dtype": "u8", "data": {"batch64": "synthetic (seeded pan/object clips, 24-picture ping-pong per stream)",
                                 "stress1024": "synthetic (per-16x16-block random motion in [-15,15] plus noise, "
                                               "24-picture ping-pong per stream)"}[args.workload],
-        "config": {"workload": args.workload, "streams": len(streams), "mb_per_step": mb_per_step,
-                   "me_mode": ("full (every vector of [-15,15]^2; not bit-exact to the reference)" if me_mode
-                               else "reference (11x11 grid + 7x7 refinement)"),
-                   "l2": "flushed before every timed step (256 MiB write)", "parallelism": f"sessions x{world}"},
+        "config": workload_config(args, streams, mb_per_step, world),
         "kernels_ms": {"encode": mean_kernel, "bitstream": float(np.mean(bits_ms))},
         "bitstream_bytes_per_step": float(np.mean(bits_bytes)),
         "e2e": {"value": e2e, "unit": "MB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -543,10 +672,17 @@ def ours(args, world, rank, local, dist):
                 "l2": "not flushed (steady pipeline: inputs arrive from the host each step)",
                 "pipeline": "three steps in flight: the host reads step k-2 after issuing step k",
                 "latency_ms": {"p50": float(np.percentile(e2e_lat, 50)), "p99": float(np.percentile(e2e_lat, 99))}},
-        "pipelined_device": {"value": piped, "unit": "MB/s",
-                             "note": "pictures in HBM, steps back to back with three in flight, L2 not "
-                                     "flushed: the pace the end-to-end loop reaches when the host keeps up"},
-        "single_stream": {"value": single, "unit": "MB/s", "pictures": len(single_lat)},
+        "pipelined_device": {"value": piped, "unit": "MB/s", "steps": piped_steps,
+                             "ms_per_step": piped_s * 1e3 / piped_steps,
+                             "step_phases_ms_median": phase_ms,
+                             "note": "pictures in HBM, steps back to back with three in flight after their own "
+                                     "warm-up, L2 not flushed: the pace the end-to-end loop reaches when the "
+                                     "host keeps up; phases: upload = descriptor copy, wait = for the previous "
+                                     "step's encode, encode, bitstream = encode end to last picture written, "
+                                     "total = step begin to records downloaded"},
+        "single_stream": {"value": single, "unit": "MB/s", "pictures": len(single_lat),
+                          "note": "the batch's streams one at a time, one synchronous picture per step, after "
+                                  "an untimed stream of each size"},
         "batch_vs_single": value / single,
         # issue to bitstream on the host, each step read one step later
         "latency_ms": {"batched_p50": float(np.percentile(lat, 50)), "batched_p99": float(np.percentile(lat, 99)),
@@ -565,15 +701,124 @@ def ours(args, world, rank, local, dist):
                    "note": "steps whose launch signature repeats replay a captured CUDA graph"},
         "clocks": clk.summary(),
     }
+    line.update(extra)
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        mbs, el = cpu_baseline(streams, 3, threads)
+        warm, n = max(args.warmup, WARM_STEPS), min(args.steps, 20)
+        per_step = cpu_steps(streams, cpu_clips(streams), warm, n, threads)
+        mbs, el = sum(m for m, _ in per_step), sum(t for _, t in per_step)
         line["cpu_baseline"] = {"value": mbs / el, "unit": "MB/s", "cores": threads, "kind": "port",
-                                "sample": f"{len(streams)} streams x 3 pictures to bitstreams (oracle, C)"}
+                                "per_core": mbs / el / threads,
+                                "sample": f"{len(streams)} streams x {n} steps after {warm} untimed steps, the "
+                                          "positions the GPU arm times, to bitstreams (oracle, C, -O3)"}
     print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ------------------------------------------------- legs of the batch64 line
+
+def plain_single_stream(device, me_mode):
+    """The plain single-stream configurations through the engine, one
+    session, one synchronous picture per step (device bitstream writer;
+    the CIF stream's QUANT from the device rate control): per-picture
+    latency and MB/s, the first picture (which sets the engine up) left
+    out, as the reference CUDA's driver timing does."""
+    from h261enc_cuda_b200 import synth
+    from h261enc_cuda_b200.engine import Engine
+    out = {}
+    for name, preset, w, h, q, seed, n in PLAIN_CONFIGS:
+        clip = synth.clip(preset, w, h, seed, n)
+        ms = []
+        with Engine(device=device, max_sessions=4, levels_to_host=0, me_mode=me_mode) as e:
+            if q:
+                sid = e.open(w, h, q, bitstream=1)
+            else:
+                sid = e.open(w, h, 10, intra_period=132, bitstream=1, rate_control=1, bitrate=384000)
+            for i in range(n):
+                t = time.perf_counter()
+                e.submit_frame(sid, clip[i])
+                e.step()
+                e.sync()
+                assert e.result(sid, copy=False).bits
+                ms.append((time.perf_counter() - t) * 1e3)
+        steady = ms[1:]
+        nmb = (w // 16) * (h // 16)
+        out[name] = {"ms_per_picture_median": float(np.median(steady)), "ms_per_picture_p99":
+                     float(np.percentile(steady, 99)), "mb_per_s": nmb * len(steady) / (sum(steady) * 1e-3),
+                     "pictures": len(steady)}
+    return out
+
+
+def stress_leg(args, device, flush):
+    """The ME-heavy stress configuration on the device: 1024 QCIF streams
+    with per-block random motion, QUANT 12, one step = one picture of every
+    stream (101,376 MBs), L2 flushed before each timed step, encode and
+    bitstream kernels timed with CUDA events; with the SAD roofline
+    fraction."""
+    import torch
+    from h261enc_cuda_b200 import workloads
+    from h261enc_cuda_b200.engine import Engine, sad_peak
+    streams = workloads.stress1024()
+    clip_len = 8
+    pools = device_clips(streams, clip_len, device)
+    mb = sum(s.num_mb for s in streams)
+    with Engine(device=device, max_sessions=4 * len(streams), levels_to_host=0) as e:
+        e.reserve(176, 144, 2 * len(streams), bitstream=1)
+        run = Runner(e, streams, pools, clip_len=clip_len)
+        for _ in range(max(args.warmup, WARM_STEPS)):
+            run.queue_device()
+            e.step()
+            e.sync()
+            run.retire(run.queued - 1)
+        kms, bms = [], []
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            run.queue_device()
+            e.step()
+            kms.append(e.last_kernel_ms())
+            bms.append(e.last_bits_ms())
+            e.sync()
+            run.retire(run.queued - 1)
+    del pools
+    torch.cuda.empty_cache()
+    enc = float(np.mean(kms))
+    sad = mb * SAD_PER_MB / (enc * 1e-3)
+    peak = sad_peak(device)
+    return {"value": mb * len(kms) / ((sum(kms) + sum(bms)) * 1e-3), "unit": "MB/s", "mb_per_step": mb,
+            "steps": len(kms), "kernels_ms": {"encode": enc, "bitstream": float(np.mean(bms))},
+            "sad_roofline": {"achieved": sad, "peak": peak, "unit": "absdiff/s", "frac": sad / peak},
+            "l2": "flushed before every timed step (256 MiB write)"}
+
+
+def serving_leg(device, rank, seconds):
+    """A short serving run: Poisson arrivals at 200 sessions/s (70 % QCIF,
+    30 % CIF, 30..600 pictures at 30 per second, QUANT 4..24), admitted under
+    a 40 GB HBM budget with continuous batching; served MB/s and
+    release-to-bitstream latency per picture.  The load ramps up from zero
+    over the run (a session lasts 1..20 s)."""
+    import torch
+    from h261enc_cuda_b200 import serving
+    from h261enc_cuda_b200.engine import Engine
+    reqs = serving.poisson_requests(200.0, seconds, seed=100 + rank)
+    pool = serving.ClipPool()
+    with Engine(device=device, max_sessions=8192, levels_to_host=0, hbm_budget_bytes=40 << 30,
+                bits_host_bytes=256 << 20) as e:
+        srv = serving.Server(e, pool, fps=30.0)
+        mean_frames = (30 + 600) / 2
+        srv.plan({(176, 144): serving.expected_concurrency(200.0, mean_frames, 30.0, 0.7),
+                  (352, 288): serving.expected_concurrency(200.0, mean_frames, 30.0, 0.3)})
+        st = srv.run(reqs, duration=seconds)
+    torch.cuda.empty_cache()
+    summ = st.summary()
+    return {"value": st.macroblocks / st.duration, "unit": "MB/s", "seconds": seconds, "sessions": len(reqs),
+            "steps": st.steps, "latency_ms": summ["latency_ms"],
+            "latency_ms_second_half": summ["latency_ms_second_half"],
+            "max_concurrent_sessions": summ["max_concurrent_sessions"], "pictures": summ["pictures"],
+            "note": "Poisson 200 sessions/s from an empty server; the served rate is the offered load, "
+                    "which ramps up over the run"}
 
 
 def serve(args, world, rank, local, dist):

@@ -14,7 +14,9 @@ from ctypes import (POINTER, Structure, c_char_p, c_float, c_int8, c_int16, c_in
 import numpy as np
 
 LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
-CORE_PATH = os.path.join(LIB_DIR, "libh261b.so")
+# H261B_LIB=check loads the checking build (bounds checks in the encode
+# kernel, lib/libh261b_check.so, `make -C h261enc_cuda_b200/csrc check`)
+CORE_PATH = os.path.join(LIB_DIR, "libh261b_check.so" if os.environ.get("H261B_LIB") == "check" else "libh261b.so")
 SYNTH_PATH = os.path.join(LIB_DIR, "libh261b_synth.so")
 
 H261B_OK = 0
@@ -65,7 +67,14 @@ class EngineConfig(Structure):
     _fields_ = [("device", c_int32), ("max_sessions", c_int32), ("hbm_budget_bytes", c_int64),
                 ("me_mode", c_int32), ("fmad", c_int32), ("warps_per_cta", c_int32),
                 ("max_ctas", c_int32), ("copy_threads", c_int32), ("levels_to_host", c_int32),
-                ("bits_host_bytes", c_int64), ("use_graphs", c_int32), ("reserved", c_int32)]
+                ("bits_host_bytes", c_int64), ("use_graphs", c_int32), ("kernel_split", c_int32),
+                ("tail_items", c_int32), ("staging", c_int32), ("reserved", c_int32)]
+
+
+class LaunchPlan(Structure):
+    _fields_ = [("warps_per_cta", c_int32), ("max_ctas", c_int32), ("kernel_split", c_int32),
+                ("tail_items", c_int32), ("staging", c_int32), ("source", c_int32), ("tuning", c_int32),
+                ("reserved", c_int32)]
 
 
 class SessionConfig(Structure):
@@ -135,6 +144,8 @@ def core() -> ctypes.CDLL:
         lib.h261b_engine_submit_batch_async.argtypes = lib.h261b_engine_submit_batch.argtypes
         lib.h261b_engine_graph_stats.argtypes = [c_void_p, POINTER(c_int64), POINTER(c_int64)]
         lib.h261b_engine_launch_shape.argtypes = [c_void_p, POINTER(c_int32), POINTER(c_int32), POINTER(c_int32)]
+        lib.h261b_engine_plan.argtypes = [c_void_p, POINTER(LaunchPlan), c_int32, c_void_p, c_void_p,
+                                          POINTER(c_int32)]
         lib.h261b_engine_step_timing.argtypes = [c_void_p, POINTER(StepTiming)]
         lib.h261b_engine_last_bits_ms.argtypes = [c_void_p, POINTER(c_float)]
         lib.h261b_engine_step_pictures.argtypes = [c_void_p, c_int32, c_void_p, POINTER(c_int32),

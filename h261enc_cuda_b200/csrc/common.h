@@ -12,7 +12,30 @@
 
 #include "../../include/h261b.h"
 
+/* NVTX (header-only nvtx3): ranges cost a function-pointer check when no
+ * profiler is attached */
+#include <nvtx3/nvToolsExt.h>
+
 namespace h261b {
+
+/* a named NVTX range over a scope: the engine marks every frame-step's host
+ * work (descriptors, uploads, launches), every wait for a step and every
+ * batch of picture copies, so that a timeline shows where host time goes */
+class NvtxRange {
+  public:
+    explicit NvtxRange(const char *fmt, ...)
+    {
+        char buf[96];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        nvtxRangePushA(buf);
+    }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 void set_error(const char *fmt, ...);
 void clear_error();

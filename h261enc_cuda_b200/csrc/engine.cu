@@ -261,6 +261,42 @@ struct Session {
     Result res[NSLOT];             /* by step slot                        */
 };
 
+/* how the encode kernel is launched: the knobs of h261b_engine_config_t */
+struct LaunchPlan {
+    int32_t warps = 4;      /* warps per CTA                                 */
+    int32_t ctas = 0;       /* grid cap, 0 = one wave of resident CTAs       */
+    int32_t split = 0;      /* 0 one fused kernel, 1 search + encode kernels */
+    int32_t tail = 2;       /* items per warp drawn one at a time            */
+    int32_t staging = 0;    /* 0 16-byte cp.async, 1 bulk row copies         */
+    bool operator==(const LaunchPlan &o) const
+    {
+        return warps == o.warps && ctas == o.ctas && split == o.split && tail == o.tail && staging == o.staging;
+    }
+    /* the phases-word bits of h261b_launch_step for this plan */
+    int32_t bits() const
+    {
+        return ((tail + 1) << H261B_TAIL_SHIFT) | (staging ? H261B_STAGE_BULK : 0);
+    }
+};
+
+/* Tuning on live steps: each stage's candidates run on the engine's next
+ * mostly-inter steps (at least half of the step's MBs from inter pictures,
+ * whose search dominates), every candidate twice in round-robin order, and
+ * the one with the smallest CUDA-event time wins.  Stage 1 tries the CTA
+ * widths of the fused kernel and of the split kernels; stage 2 tries the
+ * tail length and the staging variant on the winner. */
+struct Tuner {
+    static constexpr int kRounds = 2;
+    std::vector<LaunchPlan> cands;
+    std::vector<float> best_ms;
+    size_t next = 0;          /* index into cands x kRounds                */
+    int stage = 0;            /* 1, 2 while tuning; 0 idle                  */
+    /* every candidate measured (plan, ms), for h261b_engine_tuning */
+    std::vector<std::pair<LaunchPlan, float>> log;
+    bool active() const { return stage != 0 && next < cands.size() * kRounds; }
+    const LaunchPlan &current() const { return cands[next % cands.size()]; }
+};
+
 } // namespace h261b
 
 using namespace h261b;
@@ -322,19 +358,17 @@ struct h261b_engine_s {
     bool graphs_off = false;
     int64_t graph_captures = 0, graph_replays = 0;
 
-    /* launch tuning */
-    int warps = 4, ctas = 0;
-    std::vector<std::pair<int, int>> tune_cands;
-    std::vector<float> tune_ms;
-    size_t tune_next = 0;
+    /* the encode kernel's launch plan, and its tuning */
+    LaunchPlan plan;
+    Tuner tuner;
     bool tuned = false;
     int shape_source = 0;   /* 0 configured, 1 tuned here, 2 tuned earlier in this process */
 };
 
-/* the launch shape tuning chose, per device, for the engines created after
+/* the launch plan tuning chose, per device, for the engines created after
  * it in this process */
 static std::mutex g_tuned_mu;
-static std::map<int, std::pair<int, int>> g_tuned;
+static std::map<int, LaunchPlan> g_tuned;
 
 static const char *k_version = "h261b 0.2 (sm_100a)";
 
@@ -416,12 +450,96 @@ static int sync_all(h261b_engine_t *e)
     return H261B_OK;
 }
 
+/* stage 1: CTA widths of the fused kernel and of the split kernels, for
+ * the knobs the configuration leaves open */
+static void tuner_stage1(h261b_engine_t *e)
+{
+    const h261b_engine_config_t &c = e->cfg;
+    Tuner &t = e->tuner;
+    t.cands.clear();
+    for (int split = 0; split < 2; split++) {
+        if (c.kernel_split > 0 && split != c.kernel_split - 1)
+            continue;
+        const int widths_fused[3] = { 2, 4, 8 }, widths_split[2] = { 4, 8 };
+        const int *wl = split ? widths_split : widths_fused;
+        const int nw = split ? 2 : 3;
+        for (int i = 0; i < nw; i++) {
+            if (c.warps_per_cta > 0 && wl[i] != c.warps_per_cta)
+                continue;
+            LaunchPlan p = e->plan;
+            p.split = split;
+            p.warps = wl[i];
+            t.cands.push_back(p);
+        }
+        if (c.warps_per_cta > 0 && t.cands.empty()) {
+            LaunchPlan p = e->plan;
+            p.split = split;
+            t.cands.push_back(p);
+        }
+    }
+    t.best_ms.assign(t.cands.size(), 1e30f);
+    t.next = 0;
+    t.stage = 1;
+}
+
+/* stage 2: the tail length and the staging variant on stage 1's winner */
+static void tuner_stage2(h261b_engine_t *e, const LaunchPlan &w)
+{
+    const h261b_engine_config_t &c = e->cfg;
+    Tuner &t = e->tuner;
+    t.cands.assign(1, w);
+    if (c.tail_items == 0)
+        for (int tail : { 0, 4 }) {
+            LaunchPlan p = w;
+            p.tail = tail;
+            t.cands.push_back(p);
+        }
+    if (c.staging == 0) {
+        LaunchPlan p = w;
+        p.staging = 1 - w.staging;
+        t.cands.push_back(p);
+    }
+    t.best_ms.assign(t.cands.size(), 1e30f);
+    t.next = 0;
+    t.stage = 2;
+}
+
+/* record a tuning step's time; move to the next stage or finish */
+static void tuner_record(h261b_engine_t *e, float ms)
+{
+    Tuner &t = e->tuner;
+    const size_t i = t.next % t.cands.size();
+    t.log.push_back({ t.cands[i], ms });
+    t.best_ms[i] = std::min(t.best_ms[i], ms);
+    t.next++;
+    if (t.next < t.cands.size() * Tuner::kRounds)
+        return;
+    size_t best = 0;
+    for (size_t k = 1; k < t.cands.size(); k++)
+        if (t.best_ms[k] < t.best_ms[best])
+            best = k;
+    const LaunchPlan w = t.cands[best];
+    if (t.stage == 1 && t.cands.size() >= 1 && (e->cfg.tail_items == 0 || e->cfg.staging == 0)) {
+        tuner_stage2(e, w);
+        if (t.cands.size() > 1)
+            return;
+    }
+    e->plan = w;
+    e->tuned = true;
+    e->shape_source = 1;
+    t.stage = 0;
+    std::lock_guard<std::mutex> lk(g_tuned_mu);
+    g_tuned[e->cfg.device] = w;
+}
+
 extern "C" int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engine_t **out)
 {
     clear_error();
     if (!cfg || !out || cfg->max_sessions < 1 || cfg->max_sessions > 65536 || cfg->warps_per_cta < 0 ||
         cfg->warps_per_cta > 8 || (cfg->me_mode != 0 && cfg->me_mode != 1) || cfg->copy_threads < 0 ||
-        cfg->copy_threads > 64 || cfg->bits_host_bytes < 0 || (cfg->levels_to_host != 0 && cfg->levels_to_host != 1)) {
+        cfg->copy_threads > 64 || cfg->bits_host_bytes < 0 || (cfg->levels_to_host != 0 && cfg->levels_to_host != 1) ||
+        cfg->kernel_split < 0 || cfg->kernel_split > 2 || cfg->tail_items < 0 || cfg->tail_items > 15 ||
+        cfg->staging < 0 || cfg->staging > 2) {
         set_error("h261b_engine_create: bad configuration");
         return H261B_ERR_ARG;
     }
@@ -473,29 +591,42 @@ extern "C" int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engin
                 return H261B_ERR_NOMEM;
             }
     }
-    bool cached = false;
-    if (cfg->warps_per_cta == 0) {
+    /* the launch plan: configured knobs are fixed; the others come from an
+     * earlier tuning on this device in this process, or are tuned on this
+     * engine's first mostly-inter steps */
+    LaunchPlan &pl = e->plan;
+    pl.ctas = cfg->max_ctas;
+    if (cfg->warps_per_cta > 0)
+        pl.warps = cfg->warps_per_cta;
+    if (cfg->kernel_split > 0)
+        pl.split = cfg->kernel_split - 1;
+    if (cfg->tail_items > 0)
+        pl.tail = cfg->tail_items - 1;
+    if (cfg->staging > 0)
+        pl.staging = cfg->staging - 1;
+    const bool all_set = cfg->warps_per_cta > 0 && cfg->kernel_split > 0 && cfg->tail_items > 0 && cfg->staging > 0;
+    if (all_set) {
+        e->tuned = true;
+    } else {
         std::lock_guard<std::mutex> lk(g_tuned_mu);
         auto it = g_tuned.find(cfg->device);
         if (it != g_tuned.end()) {
-            e->warps = it->second.first;
-            e->ctas = it->second.second;
+            /* a tuned plan for the knobs left open */
+            const LaunchPlan &t = it->second;
+            if (cfg->warps_per_cta == 0)
+                pl.warps = t.warps;
+            if (cfg->kernel_split == 0)
+                pl.split = t.split;
+            if (cfg->tail_items == 0)
+                pl.tail = t.tail;
+            if (cfg->staging == 0)
+                pl.staging = t.staging;
             e->tuned = true;
             e->shape_source = 2;
-            cached = true;
         }
     }
-    if (cfg->warps_per_cta > 0) {
-        e->warps = cfg->warps_per_cta;
-        e->ctas = cfg->max_ctas;
-        e->tuned = true;
-    } else if (!cached) {
-        /* launch shapes tried on the first steps: warps per CTA, each with a
-         * grid of one wave of resident CTAs */
-        const int wl[4] = { 2, 4, 8, 4 };
-        for (int w : wl)
-            e->tune_cands.push_back({ w, 0 });
-    }
+    if (!e->tuned)
+        tuner_stage1(e);
     *out = e;
     return H261B_OK;
 }
@@ -848,6 +979,7 @@ static int submit_batch(h261b_engine_t *e, int32_t n, const int32_t *ids, const 
             set_error("h261b_engine_submit_batch: NULL plane for picture %d", i);
             return H261B_ERR_ARG;
         }
+    NvtxRange range("h261b copy %d pictures%s", n, async ? " (async)" : "");
     e->copier->join();   /* one batch in flight at a time */
     std::vector<int64_t> offs((size_t)n * 3);
     uint8_t *staging = nullptr;
@@ -991,15 +1123,15 @@ extern "C" int h261b_engine_submit_device_batch(h261b_engine_t *e, int32_t n, co
     return H261B_OK;
 }
 
-static int next_launch_shape(h261b_engine_t *e, int *warps, int *ctas)
+/* the plan of the next step: a tuning candidate while the tuner runs and
+ * the step is mostly inter (returns 1), else the engine's plan */
+static int next_plan(h261b_engine_t *e, bool mostly_inter, LaunchPlan *out)
 {
-    if (!e->tuned && e->tune_next < e->tune_cands.size()) {
-        *warps = e->tune_cands[e->tune_next].first;
-        *ctas = e->tune_cands[e->tune_next].second;
+    if (!e->tuned && e->tuner.active() && mostly_inter) {
+        *out = e->tuner.current();
         return 1;
     }
-    *warps = e->warps;
-    *ctas = e->ctas;
+    *out = e->plan;
     return 0;
 }
 
@@ -1013,6 +1145,7 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
     clear_error();
     if (!e)
         return H261B_ERR_ARG;
+    NvtxRange range("h261b step %lld", (long long)e->next_step);
     cudaSetDevice(e->cfg.device);
     const int64_t id = e->next_step;
     const int p = (int)(id % NSLOT);
@@ -1037,7 +1170,7 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
                                              256) +
                                         n_list * 32,
                                     256) +
-                           levels;
+                           levels + align_up((size_t)mbs * sizeof(h261_mb_mode_decision_t), 256);
         const size_t desc = sizeof(h261b_step_dev_t) + align_up(n_list * sizeof(h261b_session_dev_t), 256) +
                             (size_t)mbs * sizeof(uint32_t);
         int rc = grow_arenas(e, p, 0, 0, res, desc);
@@ -1071,6 +1204,14 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
     const size_t ssd_base = align_up(pic_base + n * sizeof(h261b_pic_info_t), 256);
     const size_t levels_base = align_up(ssd_base + n * 32, 256);
     size_t res_off = levels_base;
+    size_t levels_total = 0;
+    for (int32_t sid : list)
+        levels_total += align_up((size_t)e->sessions[(size_t)sid].nmb * 384, 256);
+    /* the mode decisions a search launch hands to the encode launch (split
+     * kernels; device only, after the levels) */
+    const size_t md_base = levels_base + levels_total;
+    size_t md_off = md_base;
+    int64_t inter_mbs = 0;
     int32_t n_work = 0, n_bits = 0, n_rc = 0, rc_begin = 0, n_ssd = 0;
     for (size_t k = 0; k < n; k++) {
         Session &s = e->sessions[(size_t)list[k]];
@@ -1143,7 +1284,14 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
             d.md_out = s.md_dev;
             d.md_in = s.md_dev;
             n_rc++;
+        } else {
+            /* read only by an encode launch after a search launch */
+            d.md_out = (h261_mb_mode_decision_t *)(rm.dev + md_off);
+            d.md_in = d.md_out;
         }
+        md_off += (size_t)s.nmb * sizeof(h261_mb_mode_decision_t);
+        if (!intra)
+            inter_mbs += s.nmb;
     }
     /* work list: the MBs of fixed-QUANT sessions, then those of
      * rate-controlled ones (the second encode launch takes that tail) */
@@ -1161,9 +1309,19 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
     cudaStream_t st = e->stream[p];
     const size_t desc_bytes = work_off + (size_t)n_work * sizeof(uint32_t);
     e->copier->join();   /* pictures of h261b_engine_submit_batch_async */
-    int warps, ctas;
-    const int tuning = next_launch_shape(e, &warps, &ctas);
-    const int phases = H261B_PHASE_ME | H261B_PHASE_MD | H261B_PHASE_ENCDEC | (e->cfg.fmad ? 0x100 : 0);
+    LaunchPlan plan;
+    const int tuning = next_plan(e, 2 * inter_mbs >= total_mb, &plan);
+    const int warps = plan.warps, ctas = plan.ctas;
+    const int fmad_bit = e->cfg.fmad ? H261B_FMAD_BIT : 0;
+    const int phases = H261B_PHASE_ME | H261B_PHASE_MD | H261B_PHASE_ENCDEC | fmad_bit | plan.bits() |
+                       (plan.split ? H261B_KIND_SEARCH : 0);
+    if (!plan.split)
+        for (size_t k = 0; k < n; k++)
+            if (!desc[k].rc)
+            {
+                desc[k].md_out = nullptr;   /* the fused kernel hands nothing on */
+                desc[k].md_in = nullptr;
+            }
     h261b_session_dev_t *desc_dev = (h261b_session_dev_t *)(dm.dev + desc_off);
     const uint32_t *work_dev = (const uint32_t *)(dm.dev + work_off);
     const size_t upload_bytes = e->upload_checked ? e->upload_used : 0;
@@ -1193,6 +1351,9 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
         H261B_CUDA_TRY(cudaEventRecordWithFlags(e->t_ready[p], st, rf));
         H261B_CUDA_TRY(cudaEventRecordWithFlags(e->k_start[p], st, rf));
         int32_t *sched = e->sched_dev + 2 * p;
+        /* fused: one launch encodes the fixed-QUANT sessions and searches
+         * the rate-controlled ones; split: a search launch over every MB
+         * (mode decisions into md_out) */
         int lr = h261b_launch_step(desc_dev, work_dev, n_work, phases, warps, ctas, sched, st);
         if (lr == 0 && n_rc) {
             /* rate-controlled sessions: the picture QUANT from this
@@ -1203,9 +1364,17 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
             for (int q = 1; q < NSLOT && q <= id; q++)
                 H261B_CUDA_TRY(cudaStreamWaitEvent(st, e->layout_done[(id + NSLOT - q) % NSLOT], wf));
             lr = h261b_launch_ratectrl(desc_dev, (int32_t)n, st);
-            if (lr == 0)
-                lr = h261b_launch_step(desc_dev, work_dev + rc_begin, n_work - rc_begin,
-                                       H261B_PHASE_ENCDEC | (e->cfg.fmad ? 0x100 : 0), warps, ctas, sched, st);
+        }
+        if (lr == 0 && plan.split) {
+            /* the encode launch over every MB, right after the search launch
+             * (a programmatic dependent launch) or after the rate control */
+            lr = h261b_launch_step(desc_dev, work_dev, n_work,
+                                   H261B_PHASE_ENCDEC | fmad_bit | plan.bits() | H261B_KIND_ENCODE |
+                                       (n_rc ? 0 : H261B_LAUNCH_PDL),
+                                   warps, ctas, sched, st);
+        } else if (lr == 0 && n_rc) {
+            lr = h261b_launch_step(desc_dev, work_dev + rc_begin, n_work - rc_begin,
+                                   H261B_PHASE_ENCDEC | fmad_bit | plan.bits(), warps, ctas, sched, st);
         }
         if (lr != 0) {
             set_error("step launch failed: %s", cudaGetErrorString((cudaError_t)lr));
@@ -1294,21 +1463,8 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
         /* time this candidate before moving on (tuning steps are synchronous) */
         H261B_CUDA_TRY(cudaEventSynchronize(e->k_end[p]));
         float ms = 0.f;
-        cudaEventElapsedTime(&ms, e->k_start[p], e->k_end[p]);
-        e->tune_ms.push_back(ms);
-        e->tune_next++;
-        if (e->tune_next == e->tune_cands.size()) {
-            size_t best = 0;
-            for (size_t i = 1; i < e->tune_ms.size(); i++)
-                if (e->tune_ms[i] < e->tune_ms[best])
-                    best = i;
-            e->warps = e->tune_cands[best].first;
-            e->ctas = e->tune_cands[best].second;
-            e->tuned = true;
-            e->shape_source = 1;
-            std::lock_guard<std::mutex> lk(g_tuned_mu);
-            g_tuned[e->cfg.device] = { e->warps, e->ctas };
-        }
+        H261B_CUDA_TRY(cudaEventElapsedTime(&ms, e->k_start[p], e->k_end[p]));
+        tuner_record(e, ms);
     }
 
     for (int32_t sid : list) {
@@ -1325,11 +1481,19 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
     return (int)n;
 }
 
+/* Wait until every step up to `id` has completed.  Steps do not complete in
+ * issue order: step k's stream waits only for step k-1's encode kernel (its
+ * references), not for k-1's bitstream kernels and download on the other
+ * slot's stream, so each step in (done_step, id] is waited for on its own
+ * slot.  Steps older than NSLOT before the next one were waited for when
+ * their slot was reused. */
 static int wait_step(h261b_engine_t *e, int64_t id)
 {
     if (id < 0 || id <= e->done_step)
         return H261B_OK;
-    H261B_CUDA_TRY(cudaEventSynchronize(e->step_done[id % NSLOT]));
+    NvtxRange range("h261b wait step %lld", (long long)id);
+    for (int64_t k = std::max(e->done_step + 1, id - NSLOT + 1); k <= id; k++)
+        H261B_CUDA_TRY(cudaEventSynchronize(e->step_done[k % NSLOT]));
     e->done_step = id;
     reclaim(e);
     return H261B_OK;
@@ -1620,9 +1784,39 @@ extern "C" int h261b_engine_launch_shape(h261b_engine_t *e, int32_t *warps_per_c
 {
     if (!e || !warps_per_cta || !max_ctas || !source)
         return H261B_ERR_ARG;
-    *warps_per_cta = e->warps;
-    *max_ctas = e->ctas;
+    *warps_per_cta = e->plan.warps;
+    *max_ctas = e->plan.ctas;
     *source = e->shape_source;
+    return H261B_OK;
+}
+
+static h261b_launch_plan_t plan_out(const LaunchPlan &p, int32_t source, int32_t tuning)
+{
+    h261b_launch_plan_t o;
+    memset(&o, 0, sizeof(o));
+    o.warps_per_cta = p.warps;
+    o.max_ctas = p.ctas;
+    o.kernel_split = p.split + 1;
+    o.tail_items = p.tail + 1;
+    o.staging = p.staging + 1;
+    o.source = source;
+    o.tuning = tuning;
+    return o;
+}
+
+extern "C" int h261b_engine_plan(h261b_engine_t *e, h261b_launch_plan_t *plan, int32_t log_cap,
+                                 h261b_launch_plan_t *log, float *log_ms, int32_t *log_count)
+{
+    if (!e || !plan || log_cap < 0 || (log_cap > 0 && (!log || !log_ms)))
+        return H261B_ERR_ARG;
+    *plan = plan_out(e->plan, e->shape_source, e->tuned ? 0 : 1);
+    const std::vector<std::pair<LaunchPlan, float>> &lg = e->tuner.log;
+    for (size_t i = 0; i < lg.size() && (int32_t)i < log_cap; i++) {
+        log[i] = plan_out(lg[i].first, 1, 0);
+        log_ms[i] = lg[i].second;
+    }
+    if (log_count)
+        *log_count = (int32_t)lg.size();
     return H261B_OK;
 }
 

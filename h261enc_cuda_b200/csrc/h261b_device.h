@@ -135,6 +135,26 @@ typedef struct {
 #define H261B_PHASE_MD      2     /* device mode decision                   */
 #define H261B_PHASE_ENCDEC  4     /* MC, FDCT, denoise, quant, IDCT, recon  */
 
+/* the rest of h261b_launch_step's phases word:
+ *   bit 8        the reference's default-build (fused) arithmetic
+ *   bits 9-10    kernel kind: 0 fused (the phases above in one pass),
+ *                1 search (ME + MD into md_out), 2 encode (ENCDEC from md_in)
+ *   bit 11       programmatic dependent launch on the kernel before it in
+ *                the stream (an encode launch right after its search launch)
+ *   bits 12-15   tail items per warp drawn from the scheduler, plus one
+ *                (0: the default, 2)
+ */
+#define H261B_FMAD_BIT      0x100
+#define H261B_KIND_SHIFT    9
+#define H261B_KIND_SEARCH   (1 << H261B_KIND_SHIFT)
+#define H261B_KIND_ENCODE   (2 << H261B_KIND_SHIFT)
+#define H261B_LAUNCH_PDL    0x800
+#define H261B_TAIL_SHIFT    12
+/*   bit 16       stage the search window with one bulk copy per row
+ *                (cp.async.bulk, completed on a shared-memory barrier)
+ *                instead of 16-byte cp.async copies */
+#define H261B_STAGE_BULK    0x10000
+
 #ifdef __cplusplus
 extern "C" {
 #endif

@@ -64,6 +64,9 @@ constexpr uint32_t FULL = 0xffffffffu;
 
 struct __align__(16) WarpSmem {
     uint32_t buf[WIN_ROWS * WIN_PITCH_W]; /* both buffers, interleaved      */
+    uint64_t bar[2];                      /* per buffer: the barrier its bulk
+                                             row copies complete on (bulk
+                                             staging only)                   */
     float t[4][72];                       /* transpose buffer: row stride 9,
                                              block stride 72 words, so both
                                              row and column accesses of the
@@ -81,7 +84,21 @@ struct StageBuf {
     __device__ __forceinline__ const uint32_t *curc(int j) const { return p + (16 + j) * WIN_PITCH_W + SRC_COL_W; }
 };
 
-__device__ __forceinline__ StageBuf stage_view(const WarpSmem &w, int k) { return StageBuf{ w.buf + 16 * k }; }
+__device__ __forceinline__ StageBuf stage_view(const uint32_t *wbuf, int k) { return StageBuf{ wbuf + 16 * k }; }
+
+/* shared memory of one warp: both staging buffers, plus the transpose
+ * buffer for kernels that encode (the search-only kernel has none) */
+constexpr size_t kSearchWarpBytes = sizeof(uint32_t) * WIN_ROWS * WIN_PITCH_W + 2 * sizeof(uint64_t);
+static_assert(kSearchWarpBytes % 16 == 0 && offsetof(WarpSmem, t) == kSearchWarpBytes, "warp shared layout");
+
+/* what a launch of the step kernel does per MB */
+enum StepKind {
+    KIND_FUSED = 0,    /* the phases the launch asks for, in one pass       */
+    KIND_SEARCH = 1,   /* search, costs and mode decision (into md_out)     */
+    KIND_ENCODE = 2,   /* MC ... reconstruction from md_in, after a search
+                          launch (programmatic dependent launch: waits for
+                          that grid before it reads anything)               */
+};
 
 /* the coarse grid's offsets { -14, -11, -8, -5, -2, 0, 2, 5, 8, 11, 14 }
  * (megpu_kernels.cuh:27-166), by arithmetic: lanes index it at 11 places
@@ -94,6 +111,40 @@ __device__ __forceinline__ int stage1_offset(int t)
 __constant__ float c_fwd_post[8] = { 1.0, 0.720960, 0.765367, 0.850430, 1.0, 1.272759, 1.847759, 3.624510 };
 __constant__ float c_inv_pre[8] = { 1.0, 1.387040, 1.306563, 1.175876, 1.0, 0.785695, 0.541196, 0.275899 };
 __constant__ float c_inv_quant[32];
+
+/* ------------------------------------------------ debug bounds checks
+ *
+ * Built with -DH261B_DEBUG_CHECKS (make check: lib/libh261b_check.so),
+ * every global access whose address depends on a vector, a work item or a
+ * picture size, and the shared-memory window reads of the motion
+ * compensation, first test their index: a failing test is counted and its
+ * site and index recorded (h261b_debug_check_status), and the access is
+ * skipped or its index clamped into the buffer.  In the normal build the
+ * checks compile to nothing. */
+enum CheckSite {
+    CHK_WORK_ITEM = 1,      /* MB index of a work item inside its picture     */
+    CHK_STAGE_WINDOW = 2,   /* a staged window chunk inside the reference     */
+    CHK_STAGE_SOURCE = 3,   /* a staged source row inside the picture         */
+    CHK_MC_WINDOW = 4,      /* luma prediction rows inside the staged window  */
+    CHK_MC_CHROMA = 5,      /* chroma prediction rows inside the reference    */
+    CHK_RECON = 6,          /* reconstruction row inside the output picture   */
+};
+
+#ifdef H261B_DEBUG_CHECKS
+__device__ unsigned long long g_check_count;
+__device__ int g_check_first[2];
+
+__device__ __noinline__ void check_fail(int site, int value)
+{
+    if (atomicAdd(&g_check_count, 1ull) == 0) {
+        g_check_first[0] = site;
+        g_check_first[1] = value;
+    }
+}
+#define H261B_CHECK(cond, site, value) ((cond) ? true : (check_fail((site), (int)(value)), false))
+#else
+#define H261B_CHECK(cond, site, value) true
+#endif
 
 /* ------------------------------------------------------------ helpers */
 
@@ -169,6 +220,62 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait()
 {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+/* bulk copies (the async proxy) completed on a shared-memory barrier: the
+ * alternative staging of the search window, one copy per window row.  The
+ * source is always this GPU's own memory, and no copy is multicast. */
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_inval(uint64_t *bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_addr(bar)) : "memory");
+}
+/* the one arrival of a phase, announcing the bytes its copies will bring */
+__device__ __forceinline__ void mbar_arrive_expect(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 " selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(done)
+                 : "r"(smem_addr(bar)), "r"(parity)
+                 : "memory");
+    return done != 0;
+}
+__device__ __forceinline__ void bulk_copy(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+/* this thread's earlier generic accesses of shared memory before its later
+ * async-proxy writes (a buffer is refilled after the warp read it) */
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+/* bulk staging waits that gave up (bounded, so that nothing can hang);
+ * reported by h261b_stage_status, always 0 in a correct run */
+__device__ unsigned int g_stage_timeouts;
+
+/* wait for a buffer's phase, at most ~2^22 polls (each try_wait may itself
+ * suspend for a while): a copy that never completes is counted, not waited
+ * for forever */
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int lane)
+{
+    for (int i = 0; i < (1 << 22); i++)
+        if (mbar_try_wait(bar, parity))
+            return true;
+    if (lane == 0)
+        atomicAdd(&g_stage_timeouts, 1u);
+    return false;
 }
 
 /* sum of |a_i - b_i| over the four bytes, added to acc: per-byte absolute
@@ -405,29 +512,57 @@ struct MbDecision {
  * of 16 and luma planes 16-byte aligned, so a chunk lies wholly inside or
  * wholly outside the picture, and one outside is zero-filled.  Lanes 0-29
  * take (row, chunk) = (lane / 3 + 10 i, lane % 3). */
-__device__ __forceinline__ void stage_mb(WarpSmem &w, int k, const h261b_session_dev_t &S, int mbx, int mby,
-                                         int lane)
+__device__ __forceinline__ void stage_mb(uint32_t *wbuf, int k, const h261b_session_dev_t &S, int mbx, int mby,
+                                         int lane, int row_lo = 0, int row_n = WIN_ROWS, uint64_t *bar = nullptr)
 {
     const int H = S.mbh * 16;
     const int x0 = mbx * 16, y0 = mby * 16;
-    uint32_t *base = w.buf + 16 * k;
-    if (lane < 30) {
+    uint32_t *base = wbuf + 16 * k;
+    if (bar) {
+        /* bulk staging: one copy per window row inside the picture, of its
+         * 16-byte chunks inside the picture (48 bytes, or 32 at a left or
+         * right picture edge), into the same pitched rows; chunks outside
+         * the picture are zeroed by plain stores.  Lane 0 arrives on the
+         * buffer's barrier announcing the bytes of all the copies. */
+        const int c_lo = mbx > 0 ? 0 : 1, c_hi = mbx < S.mbw - 1 ? 3 : 2;
+        const uint32_t row_bytes = 16u * (uint32_t)(c_hi - c_lo);
+        const int y_first = max(y0 - 15 + row_lo, 0), y_last = min(y0 - 15 + row_lo + row_n, H);
+        const uint32_t bytes = y_last > y_first ? row_bytes * (uint32_t)(y_last - y_first) : 0u;
+        fence_proxy_async();
+        if (lane == 0)
+            mbar_arrive_expect(bar, bytes);
+        for (int r = row_lo + lane; r < row_lo + row_n; r += 32) {
+            const int y = y0 - 15 + r;
+            uint32_t *dst = base + r * WIN_PITCH_W;
+            if (y >= 0 && y < H && H261B_CHECK(x0 - 16 + 16 * c_lo >= 0 && x0 - 16 + 16 * c_hi <= S.mbw * 16,
+                                               CHK_STAGE_WINDOW, x0))
+                bulk_copy(dst + 4 * c_lo, S.ref_y + (size_t)y * S.pitch_y + x0 - 16 + 16 * c_lo, row_bytes, bar);
+            const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+            for (int j = 0; j < 3; j++)
+                if (y < 0 || y >= H || j < c_lo || j >= c_hi)
+                    *reinterpret_cast<uint4 *>(dst + 4 * j) = z;
+        }
+    } else if (lane < 30) {
         const int j = lane % 3, r0 = lane / 3;
         const bool xok = j == 1 || (j == 0 ? mbx > 0 : mbx < S.mbw - 1);
         const int x = x0 - 16 + 16 * j;
         uint32_t *dst = base + 4 * j;
-        for (int r = r0; r < WIN_ROWS; r += 10) {
+        for (int r = row_lo + r0; r < row_lo + row_n; r += 10) {
             const int y = y0 - 15 + r;
-            const bool ok = xok && y >= 0 && y < H;
+            bool ok = xok && y >= 0 && y < H;
+            ok = ok && H261B_CHECK(x >= 0 && x + 16 <= S.mbw * 16, CHK_STAGE_WINDOW, x);
             cp_async16z(dst + r * WIN_PITCH_W, ok ? S.ref_y + (size_t)y * S.pitch_y + x : S.ref_y, ok);
         }
     }
     if (lane < 16) {
-        cp_async16(base + lane * WIN_PITCH_W + SRC_COL_W, S.cur_y + (size_t)(y0 + lane) * S.pitch_y + x0);
+        if (H261B_CHECK(y0 + lane < H && x0 + 16 <= S.mbw * 16, CHK_STAGE_SOURCE, y0 + lane))
+            cp_async16(base + lane * WIN_PITCH_W + SRC_COL_W, S.cur_y + (size_t)(y0 + lane) * S.pitch_y + x0);
     } else {
         const int q = lane - 16, pl = q >> 3, r = q & 7;
         const uint8_t *src = pl ? S.cur_cr : S.cur_cb;
-        cp_async8(base + (16 + q) * WIN_PITCH_W + SRC_COL_W, src + (size_t)(mby * 8 + r) * S.pitch_c + mbx * 8);
+        if (H261B_CHECK(mby * 8 + r < S.mbh * 8 && mbx * 8 + 8 <= S.mbw * 8, CHK_STAGE_SOURCE, mby * 8 + r))
+            cp_async8(base + (16 + q) * WIN_PITCH_W + SRC_COL_W,
+                      src + (size_t)(mby * 8 + r) * S.pitch_c + mbx * 8);
     }
 }
 
@@ -629,12 +764,30 @@ __device__ __forceinline__ uint32_t encdec_pass(float (*tb)[72], const StageBuf 
             const int ra_i = max(r - 1, 0), rc_i = min(r + 1, 7);
             uint2 ra, rb, rc;
             if (luma_pass) {
-                const int wr = 15 + m.mvy + by8, wc = 16 + m.mvx + bx8;
+                int wr = 15 + m.mvy + by8, wc = 16 + m.mvx + bx8;
+                /* rows wr..wr+7 of the 46-row window, byte columns wc..wc+7
+                 * with win8's three words inside the 12-word row */
+                if (!H261B_CHECK(wr >= 0 && wr + 7 < WIN_ROWS && wc >= 0 && wc <= 40, CHK_MC_WINDOW,
+                                 wr * 64 + wc)) {
+                    wr = min(max(wr, 0), WIN_ROWS - 8);
+                    wc = min(max(wc, 0), 40);
+                }
                 rb = win8(s, wr + r, wc);
                 ra = filter ? win8(s, wr + ra_i, wc) : rb;
                 rc = filter ? win8(s, wr + rc_i, wc) : rb;
             } else {
-                const int cmx = m.mvx / 2, cmy = m.mvy / 2; /* truncation toward zero */
+                int cmx = m.mvx / 2, cmy = m.mvy / 2; /* truncation toward zero */
+#ifdef H261B_DEBUG_CHECKS
+                /* rows inside the chroma plane; glob8's words (12 bytes from
+                 * the word boundary when unaligned) inside the row */
+                {
+                    const int cx = mbx * 8 + cmx, cy = mby * 8 + cmy, wc8 = S.mbw * 8;
+                    if (!H261B_CHECK(cy >= 0 && cy + 8 <= S.mbh * 8 && cx >= 0 &&
+                                         (cx & ~3) + ((cx & 3) ? 12 : 8) <= wc8,
+                                     CHK_MC_CHROMA, cy * 4096 + cx))
+                        cmx = cmy = 0;
+                }
+#endif
                 const uint8_t *g = ((b == 4) ? S.ref_cb : S.ref_cr) + (size_t)(mby * 8 + cmy) * S.pitch_c +
                                    (mbx * 8 + cmx);
                 rb = glob8(g + (size_t)r * S.pitch_c);
@@ -829,7 +982,10 @@ __device__ __forceinline__ uint32_t encdec_pass(float (*tb)[72], const StageBuf 
             dst = S.rec_y + (size_t)(mby * 16 + by8 + r) * S.pitch_y + mbx * 16 + bx8;
         else
             dst = ((b == 4) ? S.rec_cb : S.rec_cr) + (size_t)(mby * 8 + r) * S.pitch_c + mbx * 8;
-        *reinterpret_cast<uint2 *>(dst) = make_uint2(lo, hi);
+        if (H261B_CHECK(luma_pass ? (mby * 16 + by8 + r < S.mbh * 16 && mbx * 16 + bx8 + 8 <= S.mbw * 16)
+                                  : (mby * 8 + r < S.mbh * 8 && mbx * 8 + 8 <= S.mbw * 8),
+                        CHK_RECON, mby * 4096 + mbx))
+            *reinterpret_cast<uint2 *>(dst) = make_uint2(lo, hi);
         if (S.ssd_out) {
             /* squared error of this row against the source, for the
              * picture's PSNR (h261_main.c:38-91) */
@@ -902,6 +1058,11 @@ __device__ __forceinline__ void publish_run(const h261b_session_dev_t &S, int t,
 #ifndef H261B_STEP_MIN_BLOCKS
 #define H261B_STEP_MIN_BLOCKS 2
 #endif
+/* the search-only kernel keeps neither the transforms' registers nor the
+ * transpose buffer, so more of its CTAs fit an SM */
+#ifndef H261B_SEARCH_MIN_BLOCKS
+#define H261B_SEARCH_MIN_BLOCKS 3
+#endif
 
 /* Work items are handed out in two parts.  Warp w first takes the static
  * run [w * chunk, (w + 1) * chunk) of the first total_warps * chunk items
@@ -912,17 +1073,42 @@ __device__ __forceinline__ void publish_run(const h261b_session_dev_t &S, int t,
  * take more of the tail; every warp makes exactly one fetch past the end,
  * and the last warp to finish (sched[1]) zeroes both counters for the next
  * launch.  Without a scheduler the static runs cover every item. */
-template <int FMAD>
-__global__ void __launch_bounds__(256, H261B_STEP_MIN_BLOCKS)
+template <int FMAD, int KIND>
+__global__ void __launch_bounds__(256, KIND == KIND_SEARCH ? H261B_SEARCH_MIN_BLOCKS : H261B_STEP_MIN_BLOCKS)
     step_kernel(const h261b_session_dev_t *__restrict__ sessions, const uint32_t *__restrict__ work, int32_t n_work,
-                int32_t chunk, int32_t phases, int32_t *sched)
+                int32_t chunk, int32_t phases_arg, int32_t *sched)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    /* the bitstream kernel after this one may launch now; it waits for the
-     * whole grid before it reads anything (griddepcontrol.wait) */
+    /* the kernel after this one (the encode launch after a search launch,
+     * or the bitstream kernel) may launch now; it waits for the whole grid
+     * before it reads anything (griddepcontrol.wait) */
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    /* an encode launch reads the mode decisions of the search launch before
+     * it: wait for that grid and its writes (a no-op when launched without
+     * the programmatic dependency) */
+    if (KIND == KIND_ENCODE)
+        asm volatile("griddepcontrol.wait;" ::: "memory");
+    const int phases = KIND == KIND_SEARCH   ? (H261B_PHASE_ME | H261B_PHASE_MD)
+                       : KIND == KIND_ENCODE ? H261B_PHASE_ENCDEC
+                                             : phases_arg;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    WarpSmem &sm = reinterpret_cast<WarpSmem *>(smem_raw)[warp];
+    const size_t warp_bytes = KIND == KIND_SEARCH ? kSearchWarpBytes : sizeof(WarpSmem);
+    unsigned char *mine = smem_raw + warp * warp_bytes;
+    uint32_t *wbuf = reinterpret_cast<uint32_t *>(mine);
+    float(*tb)[72] = reinterpret_cast<WarpSmem *>(mine)->t;   /* not used by KIND_SEARCH */
+    /* bulk staging: the two buffers' barriers, their phase parities, and
+     * whether a wait gave up (then the barriers are left as they are) */
+    uint64_t *bars = (phases_arg & H261B_STAGE_BULK) ? reinterpret_cast<WarpSmem *>(mine)->bar : nullptr;
+    uint32_t parity = 0;
+    bool bars_ok = true;
+    if (bars) {
+        if (lane == 0) {
+            mbar_init(&bars[0]);
+            mbar_init(&bars[1]);
+            asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        }
+        __syncwarp();
+    }
     const int warps = blockDim.x >> 5;
     const int total_warps = gridDim.x * warps;
     const int n_static = sched ? min(n_work, total_warps * chunk) : n_work;
@@ -941,13 +1127,26 @@ __global__ void __launch_bounds__(256, H261B_STEP_MIN_BLOCKS)
         return min(__shfl_sync(FULL, v, 0), n_work);
     };
     const bool want_enc = (phases & H261B_PHASE_ENCDEC) != 0;
+    /* start the copies of a work item's inputs into buffer k: the whole
+     * search window, or for an encode launch only the 16 window rows its
+     * prediction block covers (none for an intra MB) */
+    auto stage_item = [&](int k, uint32_t it) {
+        const h261b_session_dev_t &N = sessions[it >> 12];
+        const int nmb = (int)(it & 0xFFFu), nmby = nmb / N.mbw;
+        uint64_t *bar = bars ? &bars[k] : nullptr;
+        if (KIND == KIND_ENCODE) {
+            const h261_mb_mode_decision_t &d = N.md_in[nmb];
+            const bool inter = d.i_mb_type != H261B_MB_TYPE_INTRA;
+            stage_mb(wbuf, k, N, nmb - nmby * N.mbw, nmby, lane, 15 + d.i_mv_y, inter ? 16 : 0, bar);
+        } else {
+            stage_mb(wbuf, k, N, nmb - nmby * N.mbw, nmby, lane, 0, WIN_ROWS, bar);
+        }
+    };
 
     int g = next_item();
     uint32_t item = g < n_work ? work[g] : 0u;
     if (g < n_work) {
-        const h261b_session_dev_t &S = sessions[item >> 12];
-        const int mb = (int)(item & 0xFFFu), mby = mb / S.mbw;
-        stage_mb(sm, 0, S, mb - mby * S.mbw, mby, lane);
+        stage_item(0, item);
         cp_async_commit();
     }
     /* the item after g, known one MB ahead of its staging */
@@ -964,21 +1163,32 @@ __global__ void __launch_bounds__(256, H261B_STEP_MIN_BLOCKS)
         const int gnn = gn < n_work ? next_item() : n_work;
         const uint32_t nnitem = gnn < n_work ? work[gnn] : 0u;
         if (gn < n_work) {
-            const h261b_session_dev_t &N = sessions[nitem >> 12];
-            const int nmb = (int)(nitem & 0xFFFu), nmby = nmb / N.mbw;
-            stage_mb(sm, cur ^ 1, N, nmb - nmby * N.mbw, nmby, lane);
+            stage_item(cur ^ 1, nitem);
             cp_async_commit();
             cp_async_wait<1>();
         } else {
             cp_async_wait<0>();
+        }
+        if (bars) {
+            bars_ok = mbar_wait_bounded(&bars[cur], (parity >> cur) & 1u, lane) && bars_ok;
+            parity ^= 1u << cur;
         }
         __syncwarp();
 
         const int sidx = (int)(item >> 12);
         const h261b_session_dev_t &S = sessions[sidx];
         const int mb = (int)(item & 0xFFFu);
+        if (!H261B_CHECK(mb < S.mbw * S.mbh, CHK_WORK_ITEM, (int)item)) {
+            /* an item past its picture: nothing of it is read or written */
+            __syncwarp();
+            g = gn;
+            item = nitem;
+            gn = gnn;
+            nitem = nnitem;
+            continue;
+        }
         const int mby = mb / S.mbw, mbx = mb - mby * S.mbw;
-        const StageBuf b = stage_view(sm, cur);
+        const StageBuf b = stage_view(wbuf, cur);
         const bool do_me = (phases & H261B_PHASE_ME) && !S.skip_search;
 
         me_gpu_mb_t me;
@@ -1056,8 +1266,8 @@ __global__ void __launch_bounds__(256, H261B_STEP_MIN_BLOCKS)
                 quant += S.md_in[mb].i_quantiser_adjust;
             quant = min(31, max(1, quant)); /* gpu_device.cu:625-627 */
             uint32_t ssd_l = 0, ssd_c = 0;
-            uint32_t cbp = encdec_pass<FMAD>(sm.t, b, S, mb, mbx, mby, m, quant, true, lane, colsum, ssd_l);
-            cbp |= encdec_pass<FMAD>(sm.t, b, S, mb, mbx, mby, m, quant, false, lane, colsum, ssd_c);
+            uint32_t cbp = encdec_pass<FMAD>(tb, b, S, mb, mbx, mby, m, quant, true, lane, colsum, ssd_l);
+            cbp |= encdec_pass<FMAD>(tb, b, S, mb, mbx, mby, m, quant, false, lane, colsum, ssd_c);
             if (S.ssd_out) {
                 const uint32_t ey = __reduce_add_sync(FULL, ssd_l);
                 const uint32_t ecb = __reduce_add_sync(FULL, lane < 8 ? ssd_c : 0u);
@@ -1106,6 +1316,10 @@ __global__ void __launch_bounds__(256, H261B_STEP_MIN_BLOCKS)
     }
     if (want_enc && run_n > 0)
         publish_run(sessions[run_s], run_t, run_n, colsum, lane);
+    if (bars && bars_ok && lane == 0) {
+        mbar_inval(&bars[0]);
+        mbar_inval(&bars[1]);
+    }
     if (sched && lane == 0) {
         __threadfence();
         if (atomicAdd(&sched[1], 1) == total_warps - 1) {
@@ -1116,6 +1330,44 @@ __global__ void __launch_bounds__(256, H261B_STEP_MIN_BLOCKS)
 }
 
 } // namespace
+
+extern "C" int h261b_debug_check_status(int32_t *enabled, int64_t *violations, int32_t *first_site,
+                                        int32_t *first_value)
+{
+    if (!enabled || !violations || !first_site || !first_value)
+        return H261B_ERR_ARG;
+    *violations = 0;
+    *first_site = *first_value = 0;
+#ifdef H261B_DEBUG_CHECKS
+    *enabled = 1;
+    unsigned long long n = 0;
+    int first[2] = { 0, 0 };
+    const unsigned long long zero = 0;
+    if (cudaMemcpyFromSymbol(&n, g_check_count, sizeof(n)) != cudaSuccess ||
+        cudaMemcpyFromSymbol(first, g_check_first, sizeof(first)) != cudaSuccess ||
+        cudaMemcpyToSymbol(g_check_count, &zero, sizeof(zero)) != cudaSuccess)
+        return H261B_ERR_CUDA;
+    *violations = (int64_t)n;
+    *first_site = first[0];
+    *first_value = first[1];
+#else
+    *enabled = 0;
+#endif
+    return H261B_OK;
+}
+
+extern "C" int h261b_stage_status(int64_t *timeouts)
+{
+    if (!timeouts)
+        return H261B_ERR_ARG;
+    unsigned int n = 0;
+    const unsigned int zero = 0;
+    if (cudaMemcpyFromSymbol(&n, g_stage_timeouts, sizeof(n)) != cudaSuccess ||
+        cudaMemcpyToSymbol(g_stage_timeouts, &zero, sizeof(zero)) != cudaSuccess)
+        return H261B_ERR_CUDA;
+    *timeouts = (int64_t)n;
+    return H261B_OK;
+}
 
 extern "C" int h261b_set_quant_table(void)
 {
@@ -1128,6 +1380,21 @@ extern "C" int h261b_set_quant_table(void)
     return (int)cudaMemcpyToSymbol(c_inv_quant, tab, sizeof(tab));
 }
 
+namespace {
+
+using StepFn = void (*)(const h261b_session_dev_t *, const uint32_t *, int32_t, int32_t, int32_t, int32_t *);
+
+StepFn step_fn(int fmad, int kind)
+{
+    static const StepFn fns[2][3] = { { step_kernel<0, KIND_FUSED>, step_kernel<0, KIND_SEARCH>,
+                                        step_kernel<0, KIND_ENCODE> },
+                                      { step_kernel<1, KIND_FUSED>, step_kernel<1, KIND_SEARCH>,
+                                        step_kernel<1, KIND_ENCODE> } };
+    return fns[fmad][kind];
+}
+
+} // namespace
+
 extern "C" int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const uint32_t *work_dev,
                                  int32_t n_work, int32_t phases, int32_t warps_per_cta, int32_t max_ctas,
                                  int32_t *sched_dev, void *stream)
@@ -1137,11 +1404,18 @@ extern "C" int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const 
     if (warps_per_cta < 1 || warps_per_cta > 8)
         return (int)cudaErrorInvalidValue;
     const int fmad = (phases >> 8) & 1;
-    const int ph = phases & 0xFF;
+    const int kind = (phases >> H261B_KIND_SHIFT) & 3;
+    const bool pdl = (phases & H261B_LAUNCH_PDL) != 0;
+    const int tail_code = (phases >> H261B_TAIL_SHIFT) & 15;
+    if (kind > KIND_ENCODE)
+        return (int)cudaErrorInvalidValue;
+    const int ph = phases & (0xFF | H261B_STAGE_BULK);
     const int threads = warps_per_cta * 32;
-    const size_t smem = sizeof(WarpSmem) * (size_t)warps_per_cta;
+    const size_t warp_bytes = kind == KIND_SEARCH ? kSearchWarpBytes : sizeof(WarpSmem);
+    const size_t smem = warp_bytes * (size_t)warps_per_cta;
+    const StepFn fn = step_fn(fmad, kind);
     static std::mutex mu;
-    static int sms[64], resident[64][2][9];
+    static int sms[64], resident[64][2][3][9];
     int dev = 0;
     cudaError_t err = cudaGetDevice(&dev);
     if (err != cudaSuccess || dev < 0 || dev >= 64)
@@ -1153,14 +1427,15 @@ extern "C" int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const 
             if ((err = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
                 return (int)err;
             const int max_smem = (int)(sizeof(WarpSmem) * 8);
-            if ((err = cudaFuncSetAttribute(step_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)) ||
-                (err = cudaFuncSetAttribute(step_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)))
-                return (int)err;
+            for (int f = 0; f < 2; f++)
+                for (int k = 0; k < 3; k++)
+                    if ((err = cudaFuncSetAttribute(step_fn(f, k), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    max_smem)) != cudaSuccess)
+                        return (int)err;
         }
-        int &r = resident[dev][fmad][warps_per_cta];
+        int &r = resident[dev][fmad][kind][warps_per_cta];
         if (!r) {
-            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, fmad ? step_kernel<1> : step_kernel<0>, threads,
-                                                                smem);
+            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, fn, threads, smem);
             if (err != cudaSuccess)
                 return (int)err;
             r = r < 1 ? 1 : r;
@@ -1172,27 +1447,29 @@ extern "C" int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const 
     int ctas = max_ctas > 0 ? max_ctas : nsm * per_sm;
     int chunk;
     if (sched_dev) {
-        /* static runs of all but about kTailPerWarp items per warp, the rest
-         * drawn from the scheduler */
-#ifndef H261B_TAIL_PER_WARP
-#define H261B_TAIL_PER_WARP 2
-#endif
-        constexpr int kTailPerWarp = H261B_TAIL_PER_WARP;
+        /* static runs of all but about `tail` items per warp, the rest drawn
+         * from the scheduler (tail_code: tail + 1, 0 for the default 2) */
+        const int tail = tail_code ? tail_code - 1 : 2;
         ctas = (int)std::min<long long>(ctas, (n_work + warps_per_cta - 1) / warps_per_cta);
         const long long total_warps = (long long)ctas * warps_per_cta;
-        chunk = (int)std::max<long long>(0, n_work / total_warps - kTailPerWarp);
+        chunk = (int)std::max<long long>(0, n_work / total_warps - tail);
     } else {
         /* contiguous runs covering every item */
         const long long total_warps = (long long)ctas * warps_per_cta;
         chunk = (int)((n_work + total_warps - 1) / total_warps);
         ctas = (n_work + chunk * warps_per_cta - 1) / (chunk * warps_per_cta);
     }
-    cudaStream_t st = (cudaStream_t)stream;
-    if (fmad)
-        step_kernel<1><<<ctas, threads, smem, st>>>(sessions_dev, work_dev, n_work, chunk, ph, sched_dev);
-    else
-        step_kernel<0><<<ctas, threads, smem, st>>>(sessions_dev, work_dev, n_work, chunk, ph, sched_dev);
-    return (int)cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)ctas);
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = (cudaStream_t)stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return (int)cudaLaunchKernelEx(&cfg, fn, sessions_dev, work_dev, n_work, chunk, ph, sched_dev);
 }
 
 /* ------------------------------------------------ SAD primitive peak */

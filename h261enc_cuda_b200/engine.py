@@ -53,7 +53,7 @@ class Engine:
     def __init__(self, device: int = 0, max_sessions: int = 4096, hbm_budget_bytes: int = 0,
                  me_mode: int = 0, fmad: int = 1, warps_per_cta: int = 0, max_ctas: int = 0,
                  copy_threads: int = 0, levels_to_host: int = 1, bits_host_bytes: int = 0,
-                 use_graphs: int = 1):
+                 use_graphs: int = 1, kernel_split: int = 0, tail_items: int = 0, staging: int = 0):
         lib = _lib.core()
         cfg = _lib.EngineConfig()
         lib.h261b_engine_config_default(ctypes.byref(cfg))
@@ -62,6 +62,7 @@ class Engine:
         cfg.copy_threads = copy_threads
         cfg.levels_to_host, cfg.bits_host_bytes = levels_to_host, bits_host_bytes
         cfg.use_graphs = use_graphs
+        cfg.kernel_split, cfg.tail_items, cfg.staging = kernel_split, tail_items, staging
         h = ctypes.c_void_p()
         check(lib.h261b_engine_create(ctypes.byref(cfg), ctypes.byref(h)), "h261b_engine_create")
         self._h = h
@@ -247,6 +248,20 @@ class Engine:
               "h261b_engine_launch_shape")
         return w.value, c.value, src.value
 
+    def plan(self):
+        """(the encode kernel's launch plan, [(candidate plan, encode ms)]
+        the tuner measured): plans as dicts of warps_per_cta, max_ctas,
+        kernel_split (1 fused, 2 search + encode), tail_items (n + 1),
+        staging (1 cp.async, 2 bulk rows), source, tuning."""
+        cap = 64
+        log = (_lib.LaunchPlan * cap)()
+        ms = (ctypes.c_float * cap)()
+        cur, n = _lib.LaunchPlan(), ctypes.c_int32()
+        check(_lib.core().h261b_engine_plan(self._h, ctypes.byref(cur), cap, log, ms, ctypes.byref(n)),
+              "h261b_engine_plan")
+        as_dict = lambda p: {f: getattr(p, f) for f, _ in _lib.LaunchPlan._fields_ if f != "reserved"}
+        return as_dict(cur), [(as_dict(log[i]), ms[i]) for i in range(min(n.value, cap))]
+
     def step_timing(self) -> dict:
         """Device timeline of the latest completed step, in milliseconds."""
         t = _lib.StepTiming()
@@ -323,3 +338,21 @@ def sad_peak(device: int = 0) -> float:
     if _lib.core().h261b_measure_sad_peak(device, ctypes.byref(v)) != 0:
         raise _lib.H261Error("h261b_measure_sad_peak failed")
     return v.value
+
+
+def debug_check_status():
+    """(enabled, failures since the last call, first failing site, its
+    index) of the loaded library's bounds checks: enabled only in the
+    checking build (H261B_LIB=check)."""
+    en, n, site, val = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int32()
+    check(_lib.core().h261b_debug_check_status(ctypes.byref(en), ctypes.byref(n), ctypes.byref(site),
+                                               ctypes.byref(val)), "h261b_debug_check_status")
+    return bool(en.value), n.value, site.value, val.value
+
+
+def stage_timeouts() -> int:
+    """Bulk-staging waits that gave up on the current device since the last
+    call (h261b_stage_status; 0 in every correct run)."""
+    n = ctypes.c_int64()
+    check(_lib.core().h261b_stage_status(ctypes.byref(n)), "h261b_stage_status")
+    return n.value

@@ -71,6 +71,21 @@ typedef struct {
     int32_t use_graphs;       /* 1 (default): a step whose launches look like
                                  an earlier one's (sizes, arenas, launch
                                  shape) replays that step's CUDA graph      */
+    /* Encode-kernel knobs.  0 (the default) leaves a knob to the tuner,
+     * which tries the candidates on the engine's first mostly-inter steps
+     * and keeps the fastest by CUDA-event time (per device, for the rest of
+     * the process); the output never depends on them. */
+    int32_t kernel_split;     /* 1: one kernel per step (search, mode
+                                 decision and encode fused); 2: a search
+                                 kernel (more warps per SM) and an encode
+                                 kernel chained by a programmatic dependent
+                                 launch                                      */
+    int32_t tail_items;       /* n > 0: each warp takes all but n - 1 of its
+                                 share of the work list in one static run and
+                                 draws the rest one MB at a time            */
+    int32_t staging;          /* 1: 16-byte cp.async copies of the search
+                                 window; 2: one bulk copy per window row
+                                 completed on a shared-memory barrier        */
     int32_t reserved;
 } h261b_engine_config_t;
 
@@ -279,6 +294,22 @@ int h261b_engine_graph_stats(h261b_engine_t *e, int64_t *captures, int64_t *repl
  * (0). */
 int h261b_engine_launch_shape(h261b_engine_t *e, int32_t *warps_per_cta, int32_t *max_ctas, int32_t *source);
 
+/* Every knob of the encode kernel's launch, in h261b_engine_config_t's
+ * encoding (kernel_split 1 fused / 2 search + encode, tail_items n + 1,
+ * staging 1 cp.async / 2 bulk rows). */
+typedef struct {
+    int32_t warps_per_cta, max_ctas, kernel_split, tail_items, staging;
+    int32_t source;           /* 0 configured, 1 tuned by this engine, 2 tuned
+                                 earlier in this process on this device      */
+    int32_t tuning;           /* 1 while this engine still tries candidates  */
+    int32_t reserved;
+} h261b_launch_plan_t;
+/* The engine's launch plan, and the candidates its tuner measured so far
+ * (each with its encode time in ms, in the order run; up to log_cap of them
+ * into log / log_ms, the total in *log_count). */
+int h261b_engine_plan(h261b_engine_t *e, h261b_launch_plan_t *plan, int32_t log_cap, h261b_launch_plan_t *log,
+                      float *log_ms, int32_t *log_count);
+
 /* Device time of the last step's encode kernel, and of its bitstream
  * kernel (0 without bitstream sessions), in milliseconds (CUDA events). */
 int h261b_engine_last_kernel_ms(h261b_engine_t *e, float *ms);
@@ -291,6 +322,21 @@ int h261b_engine_last_copy_bytes(h261b_engine_t *e, int64_t *h2d, int64_t *d2h);
 /* Throughput of the 4-pixel SAD primitive the motion search uses, measured
  * on the device with every SM busy: absolute differences per second. */
 int h261b_measure_sad_peak(int32_t device, double *absdiff_per_s);
+/* Bounds checks of the checking build (lib/libh261b_check.so, `make check`,
+ * compiled with H261B_DEBUG_CHECKS): every global access of the encode
+ * kernel whose address depends on a vector, a work item or a picture size,
+ * and the motion compensation's window reads, test their index first and a
+ * failing test is counted, its access skipped or clamped.  Reports whether
+ * the loaded library checks (enabled), the failures since the last call
+ * (then resets the count) and the first failure's site and index.  The
+ * normal build reports enabled = 0 and no failures. */
+int h261b_debug_check_status(int32_t *enabled, int64_t *violations, int32_t *first_site, int32_t *first_value);
+/* Waits of the bulk-copy staging (staging = 2) that gave up on the current
+ * device since the last call (then resets the count).  Every wait of the
+ * encode kernel is bounded; a wait that gives up leaves that MB's window
+ * incomplete, so a non-zero count means the step's output is wrong.  0 in
+ * every correct run. */
+int h261b_stage_status(int64_t *timeouts);
 
 /* ---- one picture, no allocation ------------------------------------------
  * No counterpart in the reference: this entry point exists for callers that
@@ -312,7 +358,9 @@ typedef struct {
     int32_t quant;            /* picture QUANT 1..31                          */
     int32_t me_mode;          /* H261B_ME_REFERENCE / H261B_ME_FULL           */
     int32_t fmad;             /* 1: the reference's default-build arithmetic  */
-    int32_t denoise;          /* strength written when reset_state is set     */
+    int32_t denoise;          /* denoise strength; read only when reset_state
+                                 is 1 (later calls keep the strength the
+                                 stream started with and ignore this field) */
     int32_t reset_state;      /* 1: first picture of a stream, clear state    */
     const uint8_t *cur_y, *cur_cb, *cur_cr;  /* device: source, pitch W / W/2 */
     const uint8_t *ref_y, *ref_cb, *ref_cr;  /* device: previous reconstruction */

@@ -260,3 +260,31 @@ def test_three_steps_in_flight_match_oracle(gpu):
         read(n - 1)
     for j, inst in enumerate(insts):
         assert bits[j] == O.encode_stream(inst.clip, inst.w, inst.h, quant=inst.q)[0], f"session {j}"
+
+
+def test_sync_waits_for_every_step_in_flight(gpu):
+    """Steps complete out of order: step k waits only for step k-1's encode
+    kernel, not for k-1's bitstream kernels and record download on its own
+    stream.  Step 0 holds 24 CIF sessions with bitstreams, step 1 only a
+    QCIF session; sync() must still leave step 0's results complete (every
+    CIF session's records and bytes equal the oracle's first picture)."""
+    n_cif = 24
+    clips = [synth.clip(2, 352, 288, 900 + k, 1) for k in range(n_cif)]
+    small = synth.clip(2, 176, 144, 950, 2)
+    with Engine(max_sessions=64, levels_to_host=1) as e:
+        big = [e.open(352, 288, 8, bitstream=1) for _ in range(n_cif)]
+        sid = e.open(176, 144, 8, bitstream=1)
+        e.submit_frames(big + [sid], [c[0] for c in clips] + [small[0]])
+        e.step()
+        e.submit_frame(sid, small[1])
+        e.step()
+        e.sync()
+        for k, b in enumerate(big):
+            want_bits, _, _, _ = O.encode_stream(clips[k], 352, 288, quant=8)
+            want = O.encode_sequence(clips[k], 352, 288, 8)
+            r = e.result(b)
+            assert r.frame_index == 0 and r.bits_status == 0
+            assert r.bits == want_bits, f"session {k}: bytes differ"
+            got = r.to_abi(352)
+            assert np.array_equal(got["tcoeff"], want["mbs"][0]["tcoeff"]), f"session {k}: levels differ"
+            assert np.array_equal(got["type"], want["mbs"][0]["type"]), f"session {k}: types differ"
