@@ -239,7 +239,7 @@ class CpuRunner:
     stream to H.261 bytes, the streams spread over a thread pool (the C
     encoder releases the GIL), largest pictures first."""
 
-    def __init__(self, streams, clips, threads, clip_len=CLIP_LEN):
+    def __init__(self, streams, clips, threads, clip_len=CLIP_LEN, keep=False):
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as O
         from h261enc_cuda_b200 import workloads
@@ -250,6 +250,8 @@ class CpuRunner:
         self.index = [workloads.clip_index(k, clip_len) for k in range(self.period)]
         self.order = sorted(range(len(streams)), key=lambda j: -streams[j].num_mb)
         self.ex = ThreadPoolExecutor(max_workers=threads)
+        # keep=True: every picture's bytes, per stream (tests)
+        self.out = [[] for _ in streams] if keep else None
         O.lib()
 
     def _one(self, j):
@@ -259,7 +261,11 @@ class CpuRunner:
                 self.enc[j].close()
             self.enc[j] = self.O.Stream(s.width, s.height, quant=s.quant)
             self.pos[j] = 0
-        self.enc[j].encode_count(self.clips[j][self.index[self.pos[j] % self.period]])
+        pic = self.clips[j][self.index[self.pos[j] % self.period]]
+        if self.out is not None:
+            self.out[j].append(self.enc[j].encode(pic))
+        else:
+            self.enc[j].encode_count(pic)
         self.pos[j] += 1
         return s.num_mb
 

@@ -13,7 +13,9 @@
 #include <condition_variable>
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <mutex>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -72,10 +74,25 @@ class CopyPool {
   public:
     static constexpr size_t kPiece = 64 << 10;
 
-    explicit CopyPool(int threads)
+    /* Starts up to `threads` workers.  A worker the system cannot start
+     * (std::system_error from thread creation) is left out: the pool runs
+     * with the ones that started, down to none, in which case the calling
+     * thread copies every batch itself.  `spawn` creates a worker thread
+     * (tests pass one that fails); `on_piece`, when set, runs in a worker
+     * before each piece it copies (tests stall a worker with it). */
+    using Spawn = std::function<std::thread(std::function<void()>)>;
+    explicit CopyPool(int threads, Spawn spawn = nullptr, std::function<void(int)> on_piece = nullptr)
+        : on_piece_(std::move(on_piece))
     {
-        for (int i = 0; i < threads; i++)
-            workers_.emplace_back([this] { loop(); });
+        if (!spawn)
+            spawn = [](std::function<void()> f) { return std::thread(std::move(f)); };
+        for (int i = 0; i < threads; i++) {
+            try {
+                workers_.push_back(spawn([this, i] { loop(i); }));
+            } catch (const std::system_error &) {
+                break;
+            }
+        }
     }
 
     ~CopyPool()
@@ -156,13 +173,16 @@ class CopyPool {
         cv_.notify_all();
     }
 
-    void work()
+    /* copy pieces until none is left; worker = -1 for a calling thread */
+    void work(int worker = -1)
     {
         const size_t n = pieces_.size();
         for (;;) {
             const size_t i = next_.fetch_add(1, std::memory_order_relaxed);
             if (i >= n)
                 return;
+            if (worker >= 0 && on_piece_)
+                on_piece_(worker);
             stream_copy(pieces_[i].dst, pieces_[i].src, pieces_[i].bytes);
             stream_fence();   /* visible before the batch counts as done */
             if (left_.fetch_sub(1, std::memory_order_acq_rel) == 1) {
@@ -172,7 +192,7 @@ class CopyPool {
         }
     }
 
-    void loop()
+    void loop(int worker)
     {
         uint64_t seen = 0;
         for (;;) {
@@ -184,13 +204,14 @@ class CopyPool {
                 seen = gen_;
                 active_++;
             }
-            work();
+            work(worker);
             std::lock_guard<std::mutex> lk(m_);
             if (--active_ == 0)
                 idle_cv_.notify_all();
         }
     }
 
+    std::function<void(int)> on_piece_;
     std::vector<std::thread> workers_;
     std::vector<CopyJob> pieces_;
     std::atomic<size_t> next_{ 0 };

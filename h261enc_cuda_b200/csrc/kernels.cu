@@ -265,14 +265,28 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
  * reported by h261b_stage_status, always 0 in a correct run */
 __device__ unsigned int g_stage_timeouts;
 
-/* wait for a buffer's phase, at most ~2^22 polls (each try_wait may itself
- * suspend for a while): a copy that never completes is counted, not waited
- * for forever */
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+/* wait for a buffer's phase for at most 100 ms of the global timer (a row
+ * copy takes about a microsecond): a copy that never completes is counted,
+ * not waited for forever, and the warp stops waiting from then on */
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int lane)
 {
-    for (int i = 0; i < (1 << 22); i++)
-        if (mbar_try_wait(bar, parity))
-            return true;
+    if (mbar_try_wait(bar, parity))
+        return true;
+    const uint64_t t0 = global_ns();
+    for (;;) {
+        for (int i = 0; i < 64; i++)
+            if (mbar_try_wait(bar, parity))
+                return true;
+        if (global_ns() - t0 > 100000000ull)
+            break;
+    }
     if (lane == 0)
         atomicAdd(&g_stage_timeouts, 1u);
     return false;
@@ -1170,7 +1184,10 @@ __global__ void __launch_bounds__(256, KIND == KIND_SEARCH ? H261B_SEARCH_MIN_BL
             cp_async_wait<0>();
         }
         if (bars) {
-            bars_ok = mbar_wait_bounded(&bars[cur], (parity >> cur) & 1u, lane) && bars_ok;
+            /* after a wait gave up, the warp waits no more (its results are
+             * wrong already and counted) */
+            if (bars_ok)
+                bars_ok = __all_sync(FULL, mbar_wait_bounded(&bars[cur], (parity >> cur) & 1u, lane));
             parity ^= 1u << cur;
         }
         __syncwarp();

@@ -5,9 +5,13 @@
 // and exits 0 on success.
 #include "copy_pool.h"
 
+#include <atomic>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <random>
+#include <system_error>
+#include <thread>
 #include <vector>
 
 using h261b::CopyJob;
@@ -88,6 +92,59 @@ int main()
         pool.join();
         if (pool.busy())
             return fail("busy after an empty batch", workers);
+    }
+    /* failures injected on the host: workers that cannot be started, and
+     * a worker that stalls in the middle of a batch */
+    for (int started : { 0, 2 }) {
+        /* thread creation fails after `started` workers (resource
+         * exhaustion): the pool keeps those and every batch still lands */
+        int made = 0;
+        CopyPool pool(6, [&](std::function<void()> f) {
+            if (made == started)
+                throw std::system_error(std::make_error_code(std::errc::resource_unavailable_try_again));
+            made++;
+            return std::thread(std::move(f));
+        });
+        if (pool.threads() != started)
+            return fail("workers after a failed start", started, pool.threads());
+        for (int i = 0; i < 6; i++) {
+            Batch b;
+            make_batch(b, rng, 8);
+            if (i % 2)
+                pool.run(b.jobs);
+            else {
+                pool.start(b.jobs);
+                pool.join();
+            }
+            if (!landed(b))
+                return fail("a batch did not land with workers missing", started, i);
+        }
+    }
+    {
+        /* worker 0 sleeps before each piece: the caller and the other
+         * workers take the rest, and run / join still return only once
+         * every byte is in place */
+        std::atomic<int> stalls{ 0 };
+        CopyPool pool(3, nullptr, [&](int w) {
+            if (w == 0) {
+                stalls++;
+                std::this_thread::sleep_for(std::chrono::milliseconds(20));
+            }
+        });
+        for (int i = 0; i < 6; i++) {
+            Batch b;
+            make_batch(b, rng, 12);
+            if (i % 2)
+                pool.run(b.jobs);
+            else {
+                pool.start(b.jobs);
+                pool.join();
+            }
+            if (!landed(b) || pool.busy())
+                return fail("a batch did not land around a stalled worker", i);
+        }
+        if (stalls.load() == 0)
+            return fail("the stalled worker never took a piece");
     }
     std::printf("ok\n");
     return 0;

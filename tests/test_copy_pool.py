@@ -1,7 +1,11 @@
 """The staging copy pool on the CPU (h261enc_cuda_b200/csrc/copy_pool.h, built
 with g++): the batches of h261b_engine_submit_batch (synchronous) and
 h261b_engine_submit_batch_async (started, then joined by the next step) land
-byte for byte, with 0 to 7 workers and pieces split across plane copies."""
+byte for byte, with 0 to 7 workers and pieces split across plane copies; and
+with failures injected on the host -- workers the system cannot start
+(the pool keeps the ones that started, down to none) and a worker that
+stalls in the middle of a batch (the others and the caller take the rest,
+and no call returns before every byte is in place)."""
 import os
 import shutil
 import subprocess

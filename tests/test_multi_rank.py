@@ -49,6 +49,54 @@ def test_two_ranks_shard_sessions_and_reduce_measurements():
         assert res[r]["max"] == 2.5 and res[r]["sum"] == 4.0
 
 
+def _encode_rank_streams(rank, steps):
+    """Rank `rank`'s batch64 streams encoded by the oracle (the bench's CPU
+    runner) for `steps` steps: the SHA-256 of every stream's bytes."""
+    import hashlib
+
+    import bench
+    from h261enc_cuda_b200 import shard, workloads
+    streams = shard.rank_streams("batch64", rank)
+    clips = [workloads.make_clip(s, steps) for s in streams]
+    run = bench.CpuRunner(streams, clips, 4, clip_len=steps, keep=True)
+    try:
+        mbs = sum(run.step()[0] for _ in range(steps))
+        return mbs, [hashlib.sha256(b"".join(pics)).hexdigest() for pics in run.out]
+    finally:
+        run.close()
+
+
+def _encoding_rank(rank, world, port, steps, out):
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "WORLD_SIZE": str(world),
+                       "RANK": str(rank), "LOCAL_RANK": str(rank)})
+    from h261enc_cuda_b200 import shard
+    dist = shard.init("gloo", timeout_s=60)
+    _, r, _ = shard.rank_info()
+    mbs, digests = _encode_rank_streams(r, steps)
+    out[r] = {"digests": digests, "total_mb": shard.sum_over_ranks(float(mbs), dist)}
+    shard.finish(dist)
+
+
+def test_two_ranks_encode_their_own_streams():
+    """Each of two gloo ranks encodes its own batch64 streams (the oracle
+    standing in for the GPU): rank r's bitstreams are exactly what one
+    process encoding rank r's streams alone writes, and the reduced MB count
+    is the sum of both ranks' work -- the data path shards with nothing
+    exchanged."""
+    world, port, steps = 2, _free_port(), 2
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_encoding_rank, args=(world, port, steps, out), nprocs=world, join=True)
+        res = dict(out)
+    mb_per_rank = (40 * 99 + 24 * 396) * steps
+    for r in (0, 1):
+        mbs, alone = _encode_rank_streams(r, steps)
+        assert mbs == mb_per_rank
+        assert res[r]["digests"] == alone, f"rank {r}: bitstreams differ from its streams encoded alone"
+        assert res[r]["total_mb"] == 2 * mb_per_rank
+    assert not set(res[0]["digests"]) & set(res[1]["digests"])
+
+
 def test_one_rank_needs_no_process_group(monkeypatch):
     from h261enc_cuda_b200 import shard
     for k in ("WORLD_SIZE", "RANK", "LOCAL_RANK"):
