@@ -607,6 +607,7 @@ def ours(args, world, rank, local, dist):
     phase_ms = {k: float(np.median([ph[k] for ph in phases])) for k in ("upload", "wait", "encode", "bitstream",
                                                                           "total")}
     graph_caps, graph_reps = eng.graph_stats()
+    plan, plan_log = eng.plan()
     eng.destroy()
 
     # ---- single stream: the same streams one at a time, one picture per
@@ -702,9 +703,15 @@ def ours(args, world, rank, local, dist):
         # the committed ncu figure is for batch64 in reference mode
         "issue_roofline": (issue_roofline(mb_per_step, mean_kernel, local, clk.summary())
                            if args.workload == "batch64" and not me_mode else None),
-        "gpu_launches": 4 * args.steps,   # encode, codes, layout, pack (which also copies)
+        # encode (search + encode when split), codes, layout, pack (which also copies)
+        "gpu_launches": (5 if plan["kernel_split"] == 2 else 4) * args.steps,
         "graphs": {"captures": graph_caps, "replays": graph_reps,
                    "note": "steps whose launch signature repeats replay a captured CUDA graph"},
+        "launch_plan": {"plan": plan, "tuning_ms": [[p["warps_per_cta"], p["kernel_split"], p["tail_items"],
+                                                      p["staging"], round(ms, 4)] for p, ms in plan_log],
+                        "note": "kernel_split 1 fused / 2 search + encode kernels; tail_items n: n - 1 MBs per "
+                                "warp drawn one at a time; staging 1 cp.async / 2 bulk rows; tuning_ms: each "
+                                "candidate's encode time on a live step (warps, split, tail, staging, ms)"},
         "clocks": clk.summary(),
     }
     line.update(extra)
@@ -737,7 +744,9 @@ def plain_single_stream(device, me_mode):
     for name, preset, w, h, q, seed, n in PLAIN_CONFIGS:
         clip = synth.clip(preset, w, h, seed, n)
         ms = []
-        with Engine(device=device, max_sessions=4, levels_to_host=0, me_mode=me_mode) as e:
+        # the host bitstream buffers are allocated with the engine (1 MiB
+        # per step slot holds any one picture), not by its first pictures
+        with Engine(device=device, max_sessions=4, levels_to_host=0, me_mode=me_mode, bits_host_bytes=1 << 20) as e:
             if q:
                 sid = e.open(w, h, q, bitstream=1)
             else:

@@ -67,7 +67,10 @@ def _run_pipelined(streams, steps, clip_len):
 
         for it in range(steps):
             before = run.sids.copy()
-            if (it // 3) % 2:
+            # alternate in blocks of 12 steps: each of the engine's three
+            # step slots then meets the same launch signature four times in
+            # a row (launched, captured, replayed twice)
+            if (it // 12) % 2:
                 run.queue_host(wait=False)
             else:
                 run.queue_device()
