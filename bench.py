@@ -85,6 +85,11 @@ def parse():
                     help="reference arm: skip timing the reference's own CUDA on the plain configurations")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the plain single-stream, stress1024 and serving legs of the batch64 line")
+    # launch-plan knobs of the encode kernel (0: tuned), h261b_engine_config_t's encoding
+    ap.add_argument("--warps", type=int, default=0, help="warps per CTA (0: tuned)")
+    ap.add_argument("--kernel-split", type=int, default=0, help="1 fused kernel, 2 search + encode kernels")
+    ap.add_argument("--tail", type=int, default=0, help="n: n - 1 tail MBs per warp drawn one at a time")
+    ap.add_argument("--staging", type=int, default=0, help="1 cp.async, 2 bulk row copies")
     ap.add_argument("--serve-seconds", type=float, default=20.0,
                     help="length of the serving run (--workload serve)")
     return ap.parse_args()
@@ -460,7 +465,9 @@ def ours(args, world, rank, local, dist):
     # every stream writes its H.261 bitstream on the device; the levels stay
     # in HBM (the bitstream is the output)
     me_mode = 1 if args.me == "full" else 0
-    eng = Engine(device=local, max_sessions=4 * len(streams), levels_to_host=0, me_mode=me_mode)
+    eng = Engine(device=local, max_sessions=4 * len(streams), levels_to_host=0, me_mode=me_mode,
+                 warps_per_cta=args.warps, kernel_split=args.kernel_split, tail_items=args.tail,
+                 staging=args.staging)
     # capacity plan: a stream that ends opens its successor while the old
     # session's last steps are in flight, so twice the sessions of each size
     # come from the pool and no session open in a timed loop allocates
