@@ -203,9 +203,14 @@ __device__ __forceinline__ void warp_range(int32_t n_work, int &lo, int &hi)
     hi = min(lo + chunk, n_work);
 }
 
+/* work items a codes warp takes per draw: an intra MB codes six blocks, a
+ * skipped inter MB none, so a static split leaves SMs idle at the end */
+constexpr int CODES_DRAW = 2;
+
 /* ---- codes: each macroblock's coefficient bit string */
 __global__ void __launch_bounds__(VLC_THREADS) codes_kernel(const h261b_session_dev_t *sessions,
-                                                            const uint32_t *work, int32_t n_work)
+                                                            const uint32_t *work, int32_t n_work,
+                                                            h261b_step_dev_t *step)
 {
     __shared__ CodesSmem sm;
     pdl_launch_dependents();
@@ -221,9 +226,20 @@ __global__ void __launch_bounds__(VLC_THREADS) codes_kernel(const h261b_session_
     __syncthreads();
 
     const int slot = lane >> 3, j = lane & 7;
-    int lo, hi;
-    warp_range(n_work, lo, hi);
-    for (int w = lo; w < hi; w++) {
+    /* the warp draws CODES_DRAW items at a time from the step's counter
+     * (zeroed by the step's descriptor upload) until the list is done */
+    int lo = 0, hi = 0;
+    for (int w = 0;; w++) {
+        if (w >= hi) {
+            int d = 0;
+            if (lane == 0)
+                d = (int)atomicAdd(&step->codes_next, (uint32_t)CODES_DRAW);
+            lo = __shfl_sync(FULL, d, 0);
+            if (lo >= n_work)
+                break;
+            hi = min(lo + CODES_DRAW, n_work);
+            w = lo;
+        }
         const uint32_t item = work[w];
         const h261b_session_dev_t &S = sessions[item >> 12];
         if (!S.bits_out)
@@ -725,7 +741,7 @@ extern "C" int h261b_launch_bitstream(h261b_session_dev_t *sessions_dev, int32_t
     const int ctas = (int)std::min<int64_t>(want, (int64_t)sm_count * pack_res);
     cudaStream_t st = (cudaStream_t)stream;
     err = launch_dependent(codes_kernel, dim3(codes_ctas), dim3(VLC_THREADS), st,
-                           (const h261b_session_dev_t *)sessions_dev, work_dev, n_work);
+                           (const h261b_session_dev_t *)sessions_dev, work_dev, n_work, step);
     if (err != cudaSuccess)
         return (int)err;
     err = launch_dependent(layout_kernel, dim3(n_sessions), dim3(LAYOUT_THREADS), st,

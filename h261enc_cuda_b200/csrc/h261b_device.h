@@ -79,7 +79,8 @@ typedef struct {
  * descriptor upload zeroes it every step) */
 typedef struct {
     uint32_t host_used;       /* bytes of the host arena handed out          */
-    uint32_t pad[63];
+    uint32_t codes_next;      /* work items the codes kernel has handed out  */
+    uint32_t pad[62];
 } h261b_step_dev_t;
 
 typedef struct {
