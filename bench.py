@@ -522,6 +522,8 @@ def ours(args, world, rank, local, dist):
     out = np.empty(64 << 20, np.uint8)
     h2d = d2h = 0
 
+    host_us = {"step": [], "queue": [], "read": []}   # host time per call, by phase
+
     def pipeline(lag, steps):
         nonlocal h2d, d2h
         lat, issued = [], []
@@ -547,15 +549,22 @@ def ours(args, world, rank, local, dist):
         first = run.queued
         run.queue_host(wait=False)
         for it in range(steps):
-            issued.append(time.perf_counter())
+            ta = time.perf_counter()
+            issued.append(ta)
             eng.step()
+            tb = time.perf_counter()
             # the next step's pictures start copying at once
             if it + 1 < steps:
                 run.queue_host(wait=False)
+            tc = time.perf_counter()
             b_in, b_out = eng.last_copy_bytes()
             h2d, d2h = h2d + b_in, d2h + b_out
             if it >= lag:
                 consume(it - lag)
+            td = time.perf_counter()
+            host_us["step"].append((tb - ta) * 1e6)
+            host_us["queue"].append((tc - tb) * 1e6)
+            host_us["read"].append((td - tc) * 1e6)
         for k in range(max(0, steps - lag), steps):
             consume(k)
         torch.cuda.synchronize()
@@ -569,7 +578,10 @@ def ours(args, world, rank, local, dist):
     # single host hiccup of a few milliseconds would otherwise weigh on a
     # loop of some 30 ms
     e2e_steps = 5 * args.steps
+    for v in host_us.values():
+        v.clear()
     e2e_wall, e2e_lat = pipeline(2, e2e_steps)
+    host_phase_us = {k: float(np.median(v)) for k, v in host_us.items()}
     e2e_s = shard.max_over_ranks(e2e_wall, dist, f"cuda:{local}")
     e2e_h2d, e2e_d2h = h2d, d2h
     _, lat = pipeline(1, min(args.steps, 100))
@@ -685,7 +697,11 @@ def ours(args, world, rank, local, dist):
                 "path": "host pictures (pageable) -> pinned arena -> HBM; records + H.261 bitstreams back",
                 "l2": "not flushed (steady pipeline: inputs arrive from the host each step)",
                 "pipeline": "three steps in flight: the host reads step k-2 after issuing step k",
-                "latency_ms": {"p50": float(np.percentile(e2e_lat, 50)), "p99": float(np.percentile(e2e_lat, 99))}},
+                "latency_ms": {"p50": float(np.percentile(e2e_lat, 50)), "p99": float(np.percentile(e2e_lat, 99))},
+                "host_us_median": host_phase_us,
+                "host_note": "per step on the host: step = h261b_engine_step (joins the picture copies, issues the "
+                             "step); queue = the next step's submission (the copies start on the engine's threads); "
+                             "read = waiting for step k-2 and moving its bitstreams out"},
         "pipelined_device": {"value": piped, "unit": "MB/s", "steps": piped_steps,
                              "ms_per_step": piped_s * 1e3 / piped_steps,
                              "step_phases_ms_median": phase_ms,
