@@ -97,6 +97,36 @@ def test_two_ranks_encode_their_own_streams():
     assert not set(res[0]["digests"]) & set(res[1]["digests"])
 
 
+def _leaving_rank(rank, world, port, out):
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "WORLD_SIZE": str(world),
+                       "RANK": str(rank), "LOCAL_RANK": str(rank)})
+    from h261enc_cuda_b200 import shard
+    dist = shard.init("gloo", timeout_s=5)
+    if rank == 1:
+        return          # leaves the job between steps, without taking its collectives
+    try:
+        shard.max_over_ranks(1.0, dist)
+        out[rank] = "no error"
+    except Exception as exc:  # the lost peer surfaces as an error, not a hang
+        out[rank] = type(exc).__name__
+
+
+def test_a_rank_that_leaves_ends_the_others_collective_with_an_error():
+    """A rank that leaves between steps (failure made on the host, no GPU
+    involved): the other rank's next measurement collective ends with an
+    error within the process group's short timeout instead of waiting for
+    good."""
+    import time
+    world, port = 2, _free_port()
+    with mp.Manager() as m:
+        out = m.dict()
+        t = time.monotonic()
+        mp.spawn(_leaving_rank, args=(world, port, out), nprocs=world, join=True)
+        res = dict(out)
+    assert res.get(0) not in (None, "no error"), res
+    assert time.monotonic() - t < 60
+
+
 def test_one_rank_needs_no_process_group(monkeypatch):
     from h261enc_cuda_b200 import shard
     for k in ("WORLD_SIZE", "RANK", "LOCAL_RANK"):
