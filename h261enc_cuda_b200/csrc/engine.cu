@@ -26,6 +26,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -358,6 +359,8 @@ struct h261b_engine_s {
     bool graphs_off = false;
     int64_t graph_captures = 0, graph_replays = 0;
 
+    /* phases-word bits the checking build adds for its tests (0 otherwise) */
+    int32_t test_bits = 0;
     /* the encode kernel's launch plan, and its tuning */
     LaunchPlan plan;
     Tuner tuner;
@@ -627,6 +630,12 @@ extern "C" int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engin
     }
     if (!e->tuned)
         tuner_stage1(e);
+#ifdef H261B_DEBUG_CHECKS
+    /* the checking build's test of the bounded staging wait: every warp's
+     * first bulk staging announces more bytes than it copies */
+    if (getenv("H261B_TEST_STAGE_SHORT"))
+        e->test_bits |= H261B_STAGE_SHORT;
+#endif
     *out = e;
     return H261B_OK;
 }
@@ -1314,7 +1323,7 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
     const int warps = plan.warps, ctas = plan.ctas;
     const int fmad_bit = e->cfg.fmad ? H261B_FMAD_BIT : 0;
     const int phases = H261B_PHASE_ME | H261B_PHASE_MD | H261B_PHASE_ENCDEC | fmad_bit | plan.bits() |
-                       (plan.split ? H261B_KIND_SEARCH : 0);
+                       e->test_bits | (plan.split ? H261B_KIND_SEARCH : 0);
     if (!plan.split)
         for (size_t k = 0; k < n; k++)
             if (!desc[k].rc)
@@ -1369,12 +1378,12 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
             /* the encode launch over every MB, right after the search launch
              * (a programmatic dependent launch) or after the rate control */
             lr = h261b_launch_step(desc_dev, work_dev, n_work,
-                                   H261B_PHASE_ENCDEC | fmad_bit | plan.bits() | H261B_KIND_ENCODE |
+                                   H261B_PHASE_ENCDEC | fmad_bit | plan.bits() | e->test_bits | H261B_KIND_ENCODE |
                                        (n_rc ? 0 : H261B_LAUNCH_PDL),
                                    warps, ctas, sched, st);
         } else if (lr == 0 && n_rc) {
             lr = h261b_launch_step(desc_dev, work_dev + rc_begin, n_work - rc_begin,
-                                   H261B_PHASE_ENCDEC | fmad_bit | plan.bits(), warps, ctas, sched, st);
+                                   H261B_PHASE_ENCDEC | fmad_bit | plan.bits() | e->test_bits, warps, ctas, sched, st);
         }
         if (lr != 0) {
             set_error("step launch failed: %s", cudaGetErrorString((cudaError_t)lr));

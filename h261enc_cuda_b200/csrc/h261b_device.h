@@ -155,6 +155,10 @@ typedef struct {
  *                (cp.async.bulk, completed on a shared-memory barrier)
  *                instead of 16-byte cp.async copies */
 #define H261B_STAGE_BULK    0x10000
+/*   bit 17       checking build only: each warp's first bulk staging
+ *                announces 16 bytes more than it copies, so that its bounded
+ *                wait runs out (the test of h261b_stage_status) */
+#define H261B_STAGE_SHORT   0x20000
 
 #ifdef __cplusplus
 extern "C" {

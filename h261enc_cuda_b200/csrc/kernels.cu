@@ -527,7 +527,8 @@ struct MbDecision {
  * wholly outside the picture, and one outside is zero-filled.  Lanes 0-29
  * take (row, chunk) = (lane / 3 + 10 i, lane % 3). */
 __device__ __forceinline__ void stage_mb(uint32_t *wbuf, int k, const h261b_session_dev_t &S, int mbx, int mby,
-                                         int lane, int row_lo = 0, int row_n = WIN_ROWS, uint64_t *bar = nullptr)
+                                         int lane, int row_lo = 0, int row_n = WIN_ROWS, uint64_t *bar = nullptr,
+                                         uint32_t extra_bytes = 0)
 {
     const int H = S.mbh * 16;
     const int x0 = mbx * 16, y0 = mby * 16;
@@ -544,7 +545,7 @@ __device__ __forceinline__ void stage_mb(uint32_t *wbuf, int k, const h261b_sess
         const uint32_t bytes = y_last > y_first ? row_bytes * (uint32_t)(y_last - y_first) : 0u;
         fence_proxy_async();
         if (lane == 0)
-            mbar_arrive_expect(bar, bytes);
+            mbar_arrive_expect(bar, bytes + extra_bytes);
         for (int r = row_lo + lane; r < row_lo + row_n; r += 32) {
             const int y = y0 - 15 + r;
             uint32_t *dst = base + r * WIN_PITCH_W;
@@ -1110,11 +1111,22 @@ __global__ void __launch_bounds__(256, KIND == KIND_SEARCH ? H261B_SEARCH_MIN_BL
     unsigned char *mine = smem_raw + warp * warp_bytes;
     uint32_t *wbuf = reinterpret_cast<uint32_t *>(mine);
     float(*tb)[72] = reinterpret_cast<WarpSmem *>(mine)->t;   /* not used by KIND_SEARCH */
-    /* bulk staging: the two buffers' barriers, their phase parities, and
-     * whether a wait gave up (then the barriers are left as they are) */
+    /* bulk staging: the two buffers' barriers; per buffer, the parity of
+     * its next phase, whether its current staging used the barrier, and
+     * whether a wait on it gave up.  A barrier whose wait gave up is not
+     * armed again (its phase may never complete): that buffer falls back to
+     * cp.async staging, and at the end the warp waits once more, bounded,
+     * for the copies of the phase that gave up. */
     uint64_t *bars = (phases_arg & H261B_STAGE_BULK) ? reinterpret_cast<WarpSmem *>(mine)->bar : nullptr;
-    uint32_t parity = 0;
-    bool bars_ok = true;
+    uint32_t parity = 0, bulk_used = 0, stuck = 0;
+#ifdef H261B_DEBUG_CHECKS
+    /* checking build only: the warp's first bulk staging announces 16 bytes
+     * more than its copies bring, so that its wait runs out (the test of the
+     * bounded wait and of h261b_stage_status) */
+    uint32_t short_first = (phases_arg & H261B_STAGE_SHORT) ? 16u : 0u;
+#else
+    const uint32_t short_first = 0u;
+#endif
     if (bars) {
         if (lane == 0) {
             mbar_init(&bars[0]);
@@ -1147,13 +1159,22 @@ __global__ void __launch_bounds__(256, KIND == KIND_SEARCH ? H261B_SEARCH_MIN_BL
     auto stage_item = [&](int k, uint32_t it) {
         const h261b_session_dev_t &N = sessions[it >> 12];
         const int nmb = (int)(it & 0xFFFu), nmby = nmb / N.mbw;
-        uint64_t *bar = bars ? &bars[k] : nullptr;
+        uint64_t *bar = (bars && !((stuck >> k) & 1u)) ? &bars[k] : nullptr;
+        const uint32_t extra = bar ? short_first : 0u;
+        if (bar) {
+            bulk_used |= 1u << k;
+#ifdef H261B_DEBUG_CHECKS
+            short_first = 0u;
+#endif
+        } else {
+            bulk_used &= ~(1u << k);
+        }
         if (KIND == KIND_ENCODE) {
             const h261_mb_mode_decision_t &d = N.md_in[nmb];
             const bool inter = d.i_mb_type != H261B_MB_TYPE_INTRA;
-            stage_mb(wbuf, k, N, nmb - nmby * N.mbw, nmby, lane, 15 + d.i_mv_y, inter ? 16 : 0, bar);
+            stage_mb(wbuf, k, N, nmb - nmby * N.mbw, nmby, lane, 15 + d.i_mv_y, inter ? 16 : 0, bar, extra);
         } else {
-            stage_mb(wbuf, k, N, nmb - nmby * N.mbw, nmby, lane, 0, WIN_ROWS, bar);
+            stage_mb(wbuf, k, N, nmb - nmby * N.mbw, nmby, lane, 0, WIN_ROWS, bar, extra);
         }
     };
 
@@ -1183,12 +1204,13 @@ __global__ void __launch_bounds__(256, KIND == KIND_SEARCH ? H261B_SEARCH_MIN_BL
         } else {
             cp_async_wait<0>();
         }
-        if (bars) {
-            /* after a wait gave up, the warp waits no more (its results are
-             * wrong already and counted) */
-            if (bars_ok)
-                bars_ok = __all_sync(FULL, mbar_wait_bounded(&bars[cur], (parity >> cur) & 1u, lane));
-            parity ^= 1u << cur;
+        if ((bulk_used >> cur) & 1u) {
+            /* a wait that gives up is counted; the buffer's barrier is not
+             * used again, so no arrival meets a phase that never ended */
+            if (!__all_sync(FULL, mbar_wait_bounded(&bars[cur], (parity >> cur) & 1u, lane)))
+                stuck |= 1u << cur;
+            else
+                parity ^= 1u << cur;
         }
         __syncwarp();
 
@@ -1333,9 +1355,17 @@ __global__ void __launch_bounds__(256, KIND == KIND_SEARCH ? H261B_SEARCH_MIN_BL
     }
     if (want_enc && run_n > 0)
         publish_run(sessions[run_s], run_t, run_n, colsum, lane);
-    if (bars && bars_ok && lane == 0) {
-        mbar_inval(&bars[0]);
-        mbar_inval(&bars[1]);
+    if (bars) {
+        for (int k = 0; k < 2; k++) {
+            /* the copies of a phase whose wait gave up may still be landing:
+             * wait for them once more, bounded, before the CTA's shared
+             * memory goes; a barrier left in a phase is not invalidated */
+            bool done = true;
+            if ((stuck >> k) & 1u)
+                done = __all_sync(FULL, mbar_wait_bounded(&bars[k], (parity >> k) & 1u, lane));
+            if (done && lane == 0)
+                mbar_inval(&bars[k]);
+        }
     }
     if (sched && lane == 0) {
         __threadfence();
@@ -1426,7 +1456,7 @@ extern "C" int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const 
     const int tail_code = (phases >> H261B_TAIL_SHIFT) & 15;
     if (kind > KIND_ENCODE)
         return (int)cudaErrorInvalidValue;
-    const int ph = phases & (0xFF | H261B_STAGE_BULK);
+    const int ph = phases & (0xFF | H261B_STAGE_BULK | H261B_STAGE_SHORT);
     const int threads = warps_per_cta * 32;
     const size_t warp_bytes = kind == KIND_SEARCH ? kSearchWarpBytes : sizeof(WarpSmem);
     const size_t smem = warp_bytes * (size_t)warps_per_cta;

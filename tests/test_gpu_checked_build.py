@@ -68,3 +68,60 @@ def test_normal_build_reports_checks_disabled():
     assert _lib.core() is not None
     en, n, _, _ = debug_check_status()
     assert not en and n == 0
+
+
+TIMEOUT_CHILD = r'''
+import json, os, sys
+import numpy as np
+sys.path.insert(0, ROOT); sys.path.insert(0, ROOT + "/oracle")
+import oracle as O
+from h261enc_cuda_b200 import synth
+from h261enc_cuda_b200.engine import Engine, stage_timeouts
+w, h, n = 176, 144, 3
+fr = synth.clip(0, w, h, 81, n)
+want = O.encode_sequence(fr, w, h, 8)
+
+def encode():
+    with Engine(warps_per_cta=4, kernel_split=1, tail_items=3, staging=2) as e:
+        sid = e.open(w, h, 8)
+        ok = True
+        for i in range(n):
+            e.submit_frame(sid, fr[i])
+            e.step()
+            e.sync()
+            ok = ok and np.array_equal(e.result(sid).to_abi(w)["tcoeff"], want["mbs"][i]["tcoeff"])
+            ok = ok and np.array_equal(np.concatenate(e.recon(sid)), want["recon"][i])
+    return ok
+
+stage_timeouts()
+forced = encode()                       # every warp's first wait runs out
+t_forced = stage_timeouts()
+del os.environ["H261B_TEST_STAGE_SHORT"]
+normal = encode()                       # a new engine in the same context
+t_normal = stage_timeouts()
+print(json.dumps({"forced_ok": bool(forced), "forced_timeouts": t_forced, "normal_ok": bool(normal),
+                  "normal_timeouts": t_normal}))
+'''
+
+
+@pytest.mark.gpu
+def test_bounded_staging_wait_runs_out_and_reports(gpu):
+    """The bulk staging's wait is bounded.  The checking build can make
+    every warp's first staging announce 16 bytes more than its copies bring
+    (H261B_TEST_STAGE_SHORT), so that the wait runs out: the kernel counts it
+    (h261b_stage_status), stops using that barrier, finishes with the data
+    the copies did bring -- the output is still the oracle's -- and the
+    context stays usable: a new engine in the same process encodes with no
+    wait running out.  No fault and no hang is made; the failure is an
+    announcement that never completes."""
+    lib = os.path.join(ROOT, "h261enc_cuda_b200", "lib", "libh261b_check.so")
+    if not os.path.exists(lib):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "h261enc_cuda_b200", "csrc"), "check"], check=True)
+    env = dict(os.environ, H261B_LIB="check", H261B_TEST_STAGE_SHORT="1")
+    r = subprocess.run([sys.executable, "-c", f"ROOT = {ROOT!r}\n" + TIMEOUT_CHILD], env=env, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    res = json.loads(r.stdout.strip().splitlines()[-1])
+    assert res["forced_timeouts"] > 0, res
+    assert res["forced_ok"], "the output changed when the staging wait ran out"
+    assert res["normal_timeouts"] == 0 and res["normal_ok"], res
