@@ -302,8 +302,10 @@ extern "C" void h261_gpu_device_me(me_gpu_t *s)
     d.frame_type = H261B_FRAME_TYPE_INTER;
     d.me_out = s->prgs_macroblocks_device;
     CK(where, cudaMemcpyAsync(g.desc_dev, &d, sizeof(d), cudaMemcpyHostToDevice, g.stream));
-    int rc = h261b_launch_step(g.desc_dev, g.work_dev, n, H261B_PHASE_ME | (g.fmad ? 0x100 : 0), 4, 0, nullptr,
-                               g.stream);
+    int rc = h261b_launch_step(g.desc_dev, g.work_dev, n,
+                               H261B_PHASE_ME | H261B_ABI_OUT | (g.me_mode ? H261B_LAUNCH_ME_FULL : 0) |
+                                   (g.fmad ? H261B_FMAD_BIT : 0),
+                               4, 0, nullptr, g.stream);
     if (rc) {
         fail(where, (cudaError_t)rc);
         return;
@@ -481,8 +483,10 @@ extern "C" void h261_gpu_device_encode_macroblocks(h261_context_t *ctx)
     d.abi_out = s->ps_macroblocks_device;
     d.frame_type = ctx->s_picture.i_frame_type;
     CK(where, cudaMemcpyAsync(g.desc_dev, &d, sizeof(d), cudaMemcpyHostToDevice, g.stream));
-    int rc = h261b_launch_step(g.desc_dev, g.work_dev, n, H261B_PHASE_ENCDEC | (g.fmad ? 0x100 : 0), 4, 0,
-                               nullptr, g.stream);
+    int rc = h261b_launch_step(g.desc_dev, g.work_dev, n,
+                               H261B_PHASE_ENCDEC | H261B_ABI_OUT | (g.me_mode ? H261B_LAUNCH_ME_FULL : 0) |
+                                   (g.fmad ? H261B_FMAD_BIT : 0),
+                               4, 0, nullptr, g.stream);
     if (rc) {
         fail(where, (cudaError_t)rc);
         return;

@@ -1321,7 +1321,9 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
     LaunchPlan plan;
     const int tuning = next_plan(e, 2 * inter_mbs >= total_mb, &plan);
     const int warps = plan.warps, ctas = plan.ctas;
-    const int fmad_bit = e->cfg.fmad ? H261B_FMAD_BIT : 0;
+    /* the arithmetic and the search mode are the engine's, for every launch */
+    const int fmad_bit =
+        (e->cfg.fmad ? H261B_FMAD_BIT : 0) | (e->cfg.me_mode == H261B_ME_FULL ? H261B_LAUNCH_ME_FULL : 0);
     const int phases = H261B_PHASE_ME | H261B_PHASE_MD | H261B_PHASE_ENCDEC | fmad_bit | plan.bits() |
                        e->test_bits | (plan.split ? H261B_KIND_SEARCH : 0);
     if (!plan.split)

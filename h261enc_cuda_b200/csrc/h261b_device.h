@@ -159,6 +159,11 @@ typedef struct {
  *                announces 16 bytes more than it copies, so that its bounded
  *                wait runs out (the test of h261b_stage_status) */
 #define H261B_STAGE_SHORT   0x20000
+/*   bit 18       the exhaustive +-15 search (the sessions' me_mode 1)
+ *   bit 19       the launch may write the reference-layout outputs
+ *                (abi_out, me_out, stage1_out: the gpu_device.h boundary) */
+#define H261B_LAUNCH_ME_FULL 0x40000
+#define H261B_ABI_OUT       0x80000
 
 #ifdef __cplusplus
 extern "C" {

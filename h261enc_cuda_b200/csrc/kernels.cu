@@ -581,7 +581,11 @@ __device__ __forceinline__ void stage_mb(uint32_t *wbuf, int k, const h261b_sess
     }
 }
 
-/* motion search + SATD costs; results are warp-uniform */
+/* motion search + SATD costs; results are warp-uniform.  FULL: the
+ * exhaustive search, else the reference's grid and refinement (a launch
+ * compiles only the one it runs: a smaller body misses the instruction
+ * cache less) */
+template <bool FULL_SEARCH>
 __device__ __forceinline__ void motion_estimate(const StageBuf s, const h261b_session_dev_t &S, int mbx, int mby,
                                                 int lane, me_gpu_mb_t &res, int8_t &s1x, int8_t &s1y)
 {
@@ -593,7 +597,7 @@ __device__ __forceinline__ void motion_estimate(const StageBuf s, const h261b_se
     /* every lane computes two SADs per iteration; a vector outside the
      * limits is replaced by (0, 0) so no address leaves the window, and its
      * cost discarded (65535, as the reference marks skipped candidates) */
-    if (S.me_mode == 1) {
+    if (FULL_SEARCH) {
         /* columns of four vertically adjacent vectors: 31 columns x 8
          * groups, the last group (vy 13..15) started at vy 12, which the
          * group before holds too (a repeated key changes no minimum) */
@@ -749,7 +753,7 @@ __device__ __forceinline__ int hfilt(uint2 v, int c)
 /* one pass over up to four blocks of the MB: lane = slot * 8 + row (then
  * column).  Adds the block-summed |coefficient| of column (lane & 7) to
  * colsum[v] and returns this pass's CBP bits. */
-template <int FMAD>
+template <int FMAD, bool ABI>
 __device__ __forceinline__ uint32_t encdec_pass(float (*tb)[72], const StageBuf s, const h261b_session_dev_t &S,
                                                 int mb, int mbx, int mby, const MbDecision &m, int quant,
                                                 bool luma_pass, int lane, int32_t colsum[8], uint32_t &ssd)
@@ -904,7 +908,7 @@ __device__ __forceinline__ uint32_t encdec_pass(float (*tb)[72], const StageBuf 
 
     /* ---- levels out */
     if (active) {
-        if (S.abi_out) {
+        if (ABI && S.abi_out) {
             int32_t *tc = S.abi_out[mb].rgi_tcoeff[b];
 #pragma unroll
             for (int v = 0; v < 8; v++)
@@ -1088,7 +1092,13 @@ __device__ __forceinline__ void publish_run(const h261b_session_dev_t &S, int t,
  * take more of the tail; every warp makes exactly one fetch past the end,
  * and the last warp to finish (sched[1]) zeroes both counters for the next
  * launch.  Without a scheduler the static runs cover every item. */
-template <int FMAD, int KIND>
+/* FMAD: the arithmetic of the reference's default build; KIND: what the
+ * launch does per MB; FULL_SEARCH: the exhaustive search instead of the
+ * reference's; ABI: the launch may write the reference-layout outputs
+ * (h261_macroblock_t records, ME results, stage-1 vectors) that only the
+ * gpu_device.h boundary asks for.  Each launch runs the instantiation for
+ * its flags (h261b_launch_step), so no launch carries code it never runs. */
+template <int FMAD, int KIND, bool FULL_SEARCH, bool ABI>
 __global__ void __launch_bounds__(256, KIND == KIND_SEARCH ? H261B_SEARCH_MIN_BLOCKS : H261B_STEP_MIN_BLOCKS)
     step_kernel(const h261b_session_dev_t *__restrict__ sessions, const uint32_t *__restrict__ work, int32_t n_work,
                 int32_t chunk, int32_t phases_arg, int32_t *sched)
@@ -1235,8 +1245,10 @@ __global__ void __launch_bounds__(256, KIND == KIND_SEARCH ? H261B_SEARCH_MIN_BL
         me.s_16x16_mv.i8_mx = me.s_16x16_mv.i8_my = 0;
         int8_t s1x = 0, s1y = 0;
         if (do_me) {
-            motion_estimate(b, S, mbx, mby, lane, me, s1x, s1y);
-            if (lane == 0) {
+            /* the launch's search mode is the session's (checking build) */
+            (void)H261B_CHECK(S.me_mode == (FULL_SEARCH ? 1 : 0), CHK_WORK_ITEM, S.me_mode);
+            motion_estimate<FULL_SEARCH>(b, S, mbx, mby, lane, me, s1x, s1y);
+            if (ABI && lane == 0) {
                 if (S.me_out)
                     S.me_out[mb] = me;
                 if (S.stage1_out) {
@@ -1305,8 +1317,8 @@ __global__ void __launch_bounds__(256, KIND == KIND_SEARCH ? H261B_SEARCH_MIN_BL
                 quant += S.md_in[mb].i_quantiser_adjust;
             quant = min(31, max(1, quant)); /* gpu_device.cu:625-627 */
             uint32_t ssd_l = 0, ssd_c = 0;
-            uint32_t cbp = encdec_pass<FMAD>(tb, b, S, mb, mbx, mby, m, quant, true, lane, colsum, ssd_l);
-            cbp |= encdec_pass<FMAD>(tb, b, S, mb, mbx, mby, m, quant, false, lane, colsum, ssd_c);
+            uint32_t cbp = encdec_pass<FMAD, ABI>(tb, b, S, mb, mbx, mby, m, quant, true, lane, colsum, ssd_l);
+            cbp |= encdec_pass<FMAD, ABI>(tb, b, S, mb, mbx, mby, m, quant, false, lane, colsum, ssd_c);
             if (S.ssd_out) {
                 const uint32_t ey = __reduce_add_sync(FULL, ssd_l);
                 const uint32_t ecb = __reduce_add_sync(FULL, lane < 8 ? ssd_c : 0u);
@@ -1321,7 +1333,7 @@ __global__ void __launch_bounds__(256, KIND == KIND_SEARCH ? H261B_SEARCH_MIN_BL
 
             const int flags = m.flags | (cbp ? H261B_MB_COEFF : 0);
             if (lane == 0) {
-                if (S.abi_out) {
+                if (ABI && S.abi_out) {
                     h261_macroblock_t *o = &S.abi_out[mb];
                     o->i_macroblock_address = 0;
                     o->i_macroblock_type = m.type;
@@ -1431,13 +1443,23 @@ namespace {
 
 using StepFn = void (*)(const h261b_session_dev_t *, const uint32_t *, int32_t, int32_t, int32_t, int32_t *);
 
-StepFn step_fn(int fmad, int kind)
+/* the instantiation of a launch's flags: the encode kind has no search and
+ * writes no reference-layout output, the search kind no encode output */
+template <int FMAD>
+StepFn step_fn_of(int kind, int full, int abi)
 {
-    static const StepFn fns[2][3] = { { step_kernel<0, KIND_FUSED>, step_kernel<0, KIND_SEARCH>,
-                                        step_kernel<0, KIND_ENCODE> },
-                                      { step_kernel<1, KIND_FUSED>, step_kernel<1, KIND_SEARCH>,
-                                        step_kernel<1, KIND_ENCODE> } };
-    return fns[fmad][kind];
+    if (kind == KIND_ENCODE)
+        return step_kernel<FMAD, KIND_ENCODE, false, false>;
+    if (kind == KIND_SEARCH)
+        return full ? step_kernel<FMAD, KIND_SEARCH, true, false> : step_kernel<FMAD, KIND_SEARCH, false, false>;
+    if (abi)
+        return full ? step_kernel<FMAD, KIND_FUSED, true, true> : step_kernel<FMAD, KIND_FUSED, false, true>;
+    return full ? step_kernel<FMAD, KIND_FUSED, true, false> : step_kernel<FMAD, KIND_FUSED, false, false>;
+}
+
+StepFn step_fn(int fmad, int kind, int full, int abi)
+{
+    return fmad ? step_fn_of<1>(kind, full, abi) : step_fn_of<0>(kind, full, abi);
 }
 
 } // namespace
@@ -1452,6 +1474,7 @@ extern "C" int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const 
         return (int)cudaErrorInvalidValue;
     const int fmad = (phases >> 8) & 1;
     const int kind = (phases >> H261B_KIND_SHIFT) & 3;
+    const int full = (phases & H261B_LAUNCH_ME_FULL) ? 1 : 0, abi = (phases & H261B_ABI_OUT) ? 1 : 0;
     const bool pdl = (phases & H261B_LAUNCH_PDL) != 0;
     const int tail_code = (phases >> H261B_TAIL_SHIFT) & 15;
     if (kind > KIND_ENCODE)
@@ -1460,9 +1483,9 @@ extern "C" int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const 
     const int threads = warps_per_cta * 32;
     const size_t warp_bytes = kind == KIND_SEARCH ? kSearchWarpBytes : sizeof(WarpSmem);
     const size_t smem = warp_bytes * (size_t)warps_per_cta;
-    const StepFn fn = step_fn(fmad, kind);
+    const StepFn fn = step_fn(fmad, kind, full, abi);
     static std::mutex mu;
-    static int sms[64], resident[64][2][3][9];
+    static int sms[64], resident[64][2][3][2][2][9];
     int dev = 0;
     cudaError_t err = cudaGetDevice(&dev);
     if (err != cudaSuccess || dev < 0 || dev >= 64)
@@ -1476,11 +1499,13 @@ extern "C" int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const 
             const int max_smem = (int)(sizeof(WarpSmem) * 8);
             for (int f = 0; f < 2; f++)
                 for (int k = 0; k < 3; k++)
-                    if ((err = cudaFuncSetAttribute(step_fn(f, k), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                    max_smem)) != cudaSuccess)
-                        return (int)err;
+                    for (int x = 0; x < 4; x++)
+                        if ((err = cudaFuncSetAttribute(step_fn(f, k, x & 1, x >> 1),
+                                                        cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)) !=
+                            cudaSuccess)
+                            return (int)err;
         }
-        int &r = resident[dev][fmad][kind][warps_per_cta];
+        int &r = resident[dev][fmad][kind][full][abi][warps_per_cta];
         if (!r) {
             err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, fn, threads, smem);
             if (err != cudaSuccess)

@@ -171,7 +171,8 @@ extern "C" int h261b_encode_picture_noalloc(const h261b_noalloc_picture_t *p, vo
     noalloc_prepare<<<1, 256, 0, st>>>(d, (h261b_session_dev_t *)scratch, (uint32_t *)p->state,
                                        p->reset_state ? 1 : 0, p->denoise);
     H261B_CUDA_TRY(cudaGetLastError());
-    const int phases = H261B_PHASE_ME | H261B_PHASE_MD | H261B_PHASE_ENCDEC | (p->fmad ? 0x100 : 0);
+    const int phases = H261B_PHASE_ME | H261B_PHASE_MD | H261B_PHASE_ENCDEC | (p->fmad ? H261B_FMAD_BIT : 0) |
+                       (p->me_mode == H261B_ME_FULL ? H261B_LAUNCH_ME_FULL : 0);
     const int lr = h261b_launch_step((const h261b_session_dev_t *)scratch,
                                      (const uint32_t *)((const uint8_t *)scratch + kDescBytes), nmb, phases, 4, 0,
                                      nullptr, st);
