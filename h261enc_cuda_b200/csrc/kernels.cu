@@ -98,6 +98,10 @@ enum StepKind {
     KIND_ENCODE = 2,   /* MC ... reconstruction from md_in, after a search
                           launch (programmatic dependent launch: waits for
                           that grid before it reads anything)               */
+    KIND_FULL = 3,     /* KIND_FUSED with every phase (search, mode decision,
+                          encode): the engine's and the no-allocation
+                          entry point's launch, compiled without the paths
+                          of partial launches                               */
 };
 
 /* the coarse grid's offsets { -14, -11, -8, -5, -2, 0, 2, 5, 8, 11, 14 }
@@ -458,11 +462,19 @@ __device__ __forceinline__ void fdct_butterfly(float tmp0, float tmp1, float tmp
     o[7] = z11 - z4;
 }
 
-/* floorf( cs * post * v + 0.49999 ): float product, double sum, float floor */
+/* floorf( cs * post * v + 0.49999 ) as the reference writes it
+ * (mbgpu_kernels.cuh:413-437): a float product, the sum with the double
+ * literal rounded to double, then to float, then the floor.  For every
+ * finite float p, floorf((float)((double)p + 0.49999)) equals
+ * floorf(p + 0.49999f) with the float literal (the float nearest to
+ * 0.49999) -- checked for all 2.5e9 floats of magnitude below 2^24 by
+ * tests/rounding_check.c; above it both leave p unchanged -- so the sum is
+ * taken in float and floored by the conversion itself: no conversion to or
+ * from double. */
 __device__ __forceinline__ int32_t fdct_round(float cs, float post, float v)
 {
     const float prod = __fmul_rn(__fmul_rn(cs, post), v);
-    return __float2int_rz(floorf(__double2float_rn(__dadd_rn((double)prod, 0.49999))));
+    return __float2int_rd(__fadd_rn(prod, 0.49999f));
 }
 
 /* the AAN inverse butterfly after its first level of adds (mbgpu_kernels.cuh
@@ -1115,6 +1127,7 @@ __global__ void __launch_bounds__(256, KIND == KIND_SEARCH ? H261B_SEARCH_MIN_BL
         asm volatile("griddepcontrol.wait;" ::: "memory");
     const int phases = KIND == KIND_SEARCH   ? (H261B_PHASE_ME | H261B_PHASE_MD)
                        : KIND == KIND_ENCODE ? H261B_PHASE_ENCDEC
+                       : KIND == KIND_FULL   ? (H261B_PHASE_ME | H261B_PHASE_MD | H261B_PHASE_ENCDEC)
                                              : phases_arg;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const size_t warp_bytes = KIND == KIND_SEARCH ? kSearchWarpBytes : sizeof(WarpSmem);
@@ -1454,6 +1467,8 @@ StepFn step_fn_of(int kind, int full, int abi)
         return full ? step_kernel<FMAD, KIND_SEARCH, true, false> : step_kernel<FMAD, KIND_SEARCH, false, false>;
     if (abi)
         return full ? step_kernel<FMAD, KIND_FUSED, true, true> : step_kernel<FMAD, KIND_FUSED, false, true>;
+    if (kind == KIND_FULL)
+        return full ? step_kernel<FMAD, KIND_FULL, true, false> : step_kernel<FMAD, KIND_FULL, false, false>;
     return full ? step_kernel<FMAD, KIND_FUSED, true, false> : step_kernel<FMAD, KIND_FUSED, false, false>;
 }
 
@@ -1473,11 +1488,15 @@ extern "C" int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const 
     if (warps_per_cta < 1 || warps_per_cta > 8)
         return (int)cudaErrorInvalidValue;
     const int fmad = (phases >> 8) & 1;
-    const int kind = (phases >> H261B_KIND_SHIFT) & 3;
+    int kind = (phases >> H261B_KIND_SHIFT) & 3;
+    /* a fused launch of every phase runs the kernel compiled for exactly that */
+    const int all_phases = H261B_PHASE_ME | H261B_PHASE_MD | H261B_PHASE_ENCDEC;
+    if (kind == KIND_FUSED && (phases & all_phases) == all_phases)
+        kind = KIND_FULL;
     const int full = (phases & H261B_LAUNCH_ME_FULL) ? 1 : 0, abi = (phases & H261B_ABI_OUT) ? 1 : 0;
     const bool pdl = (phases & H261B_LAUNCH_PDL) != 0;
     const int tail_code = (phases >> H261B_TAIL_SHIFT) & 15;
-    if (kind > KIND_ENCODE)
+    if (kind > KIND_FULL)
         return (int)cudaErrorInvalidValue;
     const int ph = phases & (0xFF | H261B_STAGE_BULK | H261B_STAGE_SHORT);
     const int threads = warps_per_cta * 32;
@@ -1485,7 +1504,7 @@ extern "C" int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const 
     const size_t smem = warp_bytes * (size_t)warps_per_cta;
     const StepFn fn = step_fn(fmad, kind, full, abi);
     static std::mutex mu;
-    static int sms[64], resident[64][2][3][2][2][9];
+    static int sms[64], resident[64][2][4][2][2][9];
     int dev = 0;
     cudaError_t err = cudaGetDevice(&dev);
     if (err != cudaSuccess || dev < 0 || dev >= 64)
@@ -1498,7 +1517,7 @@ extern "C" int h261b_launch_step(const h261b_session_dev_t *sessions_dev, const 
                 return (int)err;
             const int max_smem = (int)(sizeof(WarpSmem) * 8);
             for (int f = 0; f < 2; f++)
-                for (int k = 0; k < 3; k++)
+                for (int k = 0; k < 4; k++)
                     for (int x = 0; x < 4; x++)
                         if ((err = cudaFuncSetAttribute(step_fn(f, k, x & 1, x >> 1),
                                                         cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)) !=
