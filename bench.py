@@ -90,6 +90,8 @@ def parse():
     ap.add_argument("--kernel-split", type=int, default=0, help="1 fused kernel, 2 search + encode kernels")
     ap.add_argument("--tail", type=int, default=0, help="n: n - 1 tail MBs per warp drawn one at a time")
     ap.add_argument("--staging", type=int, default=0, help="1 cp.async, 2 bulk row copies")
+    ap.add_argument("--copy-threads", type=int, default=0,
+                    help="host threads copying pictures into the staging arena (0: the engine's default)")
     ap.add_argument("--serve-seconds", type=float, default=20.0,
                     help="length of the serving run (--workload serve)")
     return ap.parse_args()
@@ -467,7 +469,7 @@ def ours(args, world, rank, local, dist):
     me_mode = 1 if args.me == "full" else 0
     eng = Engine(device=local, max_sessions=4 * len(streams), levels_to_host=0, me_mode=me_mode,
                  warps_per_cta=args.warps, kernel_split=args.kernel_split, tail_items=args.tail,
-                 staging=args.staging)
+                 staging=args.staging, copy_threads=args.copy_threads)
     # capacity plan: a stream that ends opens its successor while the old
     # session's last steps are in flight, so twice the sessions of each size
     # come from the pool and no session open in a timed loop allocates
