@@ -220,8 +220,8 @@ def dist_setup(args):
 
 # untimed steps before either arm's timed steps (at least the --warmup
 # given): they cover the engine's tuning of its launch plan, which runs on
-# its first mostly-inter steps (18 of them)
-WARM_STEPS = 24
+# its first mostly-inter steps (27 of them)
+WARM_STEPS = 32
 
 
 def workload_config(args, streams, mb_per_step, world):

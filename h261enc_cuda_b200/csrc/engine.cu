@@ -263,11 +263,14 @@ struct Session {
 };
 
 /* how the encode kernel is launched: the knobs of h261b_engine_config_t */
+/* The defaults are the plan measured fastest on the batch64 workload; the
+ * tuner keeps them unless a candidate is clearly faster on the device at
+ * hand. */
 struct LaunchPlan {
-    int32_t warps = 4;      /* warps per CTA                                 */
+    int32_t warps = 8;      /* warps per CTA                                 */
     int32_t ctas = 0;       /* grid cap, 0 = one wave of resident CTAs       */
     int32_t split = 0;      /* 0 one fused kernel, 1 search + encode kernels */
-    int32_t tail = 2;       /* items per warp drawn one at a time            */
+    int32_t tail = 0;       /* items per warp drawn one at a time            */
     int32_t staging = 0;    /* 0 16-byte cp.async, 1 bulk row copies         */
     bool operator==(const LaunchPlan &o) const
     {
@@ -282,14 +285,18 @@ struct LaunchPlan {
 
 /* Tuning on live steps: each stage's candidates run on the engine's next
  * mostly-inter steps (at least half of the step's MBs from inter pictures,
- * whose search dominates), every candidate twice in round-robin order, and
- * the one with the smallest CUDA-event time wins.  Stage 1 tries the CTA
- * widths of the fused kernel and of the split kernels; stage 2 tries the
- * tail length and the staging variant on the winner. */
+ * whose search dominates), every candidate three times in round-robin
+ * order.  A stage keeps its incumbent (candidate 0: the default plan, then
+ * stage 1's winner) unless another candidate's median CUDA-event time is at
+ * least 3 % below the incumbent's: successive live steps differ by a few per
+ * cent in content, and a single lucky step must not move the plan.  Stage 1
+ * tries the CTA widths of the fused kernel and of the split kernels; stage 2
+ * tries the tail length and the staging variant on the winner. */
 struct Tuner {
-    static constexpr int kRounds = 2;
+    static constexpr int kRounds = 3;
+    static constexpr float kMargin = 0.97f;
     std::vector<LaunchPlan> cands;
-    std::vector<float> best_ms;
+    std::vector<std::vector<float>> ms;   /* per candidate, its rounds' times */
     size_t next = 0;          /* index into cands x kRounds                */
     int stage = 0;            /* 1, 2 while tuning; 0 idle                  */
     /* every candidate measured (plan, ms), for h261b_engine_tuning */
@@ -460,6 +467,8 @@ static void tuner_stage1(h261b_engine_t *e)
     const h261b_engine_config_t &c = e->cfg;
     Tuner &t = e->tuner;
     t.cands.clear();
+    /* candidate 0: the engine's plan (defaults and configured knobs) */
+    t.cands.push_back(e->plan);
     for (int split = 0; split < 2; split++) {
         if (c.kernel_split > 0 && split != c.kernel_split - 1)
             continue;
@@ -472,15 +481,11 @@ static void tuner_stage1(h261b_engine_t *e)
             LaunchPlan p = e->plan;
             p.split = split;
             p.warps = wl[i];
-            t.cands.push_back(p);
-        }
-        if (c.warps_per_cta > 0 && t.cands.empty()) {
-            LaunchPlan p = e->plan;
-            p.split = split;
-            t.cands.push_back(p);
+            if (!(p == t.cands[0]))
+                t.cands.push_back(p);
         }
     }
-    t.best_ms.assign(t.cands.size(), 1e30f);
+    t.ms.assign(t.cands.size(), std::vector<float>());
     t.next = 0;
     t.stage = 1;
 }
@@ -492,7 +497,9 @@ static void tuner_stage2(h261b_engine_t *e, const LaunchPlan &w)
     Tuner &t = e->tuner;
     t.cands.assign(1, w);
     if (c.tail_items == 0)
-        for (int tail : { 0, 4 }) {
+        for (int tail : { 0, 2, 4 }) {
+            if (tail == w.tail)
+                continue;
             LaunchPlan p = w;
             p.tail = tail;
             t.cands.push_back(p);
@@ -502,7 +509,7 @@ static void tuner_stage2(h261b_engine_t *e, const LaunchPlan &w)
         p.staging = 1 - w.staging;
         t.cands.push_back(p);
     }
-    t.best_ms.assign(t.cands.size(), 1e30f);
+    t.ms.assign(t.cands.size(), std::vector<float>());
     t.next = 0;
     t.stage = 2;
 }
@@ -513,14 +520,25 @@ static void tuner_record(h261b_engine_t *e, float ms)
     Tuner &t = e->tuner;
     const size_t i = t.next % t.cands.size();
     t.log.push_back({ t.cands[i], ms });
-    t.best_ms[i] = std::min(t.best_ms[i], ms);
+    t.ms[i].push_back(ms);
     t.next++;
     if (t.next < t.cands.size() * Tuner::kRounds)
         return;
+    auto median = [](std::vector<float> v) {
+        std::sort(v.begin(), v.end());
+        return v[v.size() / 2];
+    };
+    /* the incumbent (candidate 0) unless a candidate is clearly faster */
     size_t best = 0;
-    for (size_t k = 1; k < t.cands.size(); k++)
-        if (t.best_ms[k] < t.best_ms[best])
+    float best_ms = median(t.ms[0]);
+    const float bar = best_ms * Tuner::kMargin;
+    for (size_t k = 1; k < t.cands.size(); k++) {
+        const float m = median(t.ms[k]);
+        if (m < bar && m < best_ms) {
             best = k;
+            best_ms = m;
+        }
+    }
     const LaunchPlan w = t.cands[best];
     if (t.stage == 1 && t.cands.size() >= 1 && (e->cfg.tail_items == 0 || e->cfg.staging == 0)) {
         tuner_stage2(e, w);

@@ -94,7 +94,7 @@ sys.path.insert(0, ROOT); sys.path.insert(0, ROOT + "/oracle")
 import oracle as O
 from h261enc_cuda_b200 import synth
 from h261enc_cuda_b200.engine import Engine
-n, specs = 30, [(176, 144, 8, 401), (352, 288, 12, 402), (176, 144, 16, 403)]
+n, specs = 40, [(176, 144, 8, 401), (352, 288, 12, 402), (176, 144, 16, 403)]
 clips = [synth.clip(2, w, h, seed, n) for (w, h, q, seed) in specs]
 bits = [b"" for _ in specs]
 with Engine(levels_to_host=0) as e:
@@ -132,4 +132,6 @@ def test_tuner_measures_every_knob(gpu):
     assert {p["kernel_split"] for p, _ in log} == {1, 2}, log
     assert {p["staging"] for p, _ in log} == {1, 2}, log
     assert {p["tail_items"] for p, _ in log} >= {1, 3, 5}, log
+    # three rounds of every candidate: 5 in stage 1, 4 in stage 2
+    assert len(log) == 27, log
     assert all(ms > 0 for _, ms in log)
