@@ -201,7 +201,8 @@ def test_graph_replay_equals_direct_launches(gpu, preset):
     out = {}
     for graphs in (0, 1):
         got = []
-        with Engine(warps_per_cta=4, use_graphs=graphs) as e:
+        # every knob fixed: no tuning steps (which launch directly)
+        with Engine(warps_per_cta=4, kernel_split=1, tail_items=1, staging=1, use_graphs=graphs) as e:
             sids = [e.open(w, h, q, bitstream=1, rate_control=1 if b else 0, bitrate=b) for (w, h, q, b) in specs]
             for i in range(clips[0].shape[0]):
                 e.submit_frames(sids, [c[i] for c in clips])
@@ -222,17 +223,22 @@ def test_graph_replay_equals_direct_launches(gpu, preset):
 
 
 def test_tuned_launch_shape_is_reused_by_later_engines(gpu):
-    fr = synth.clip(0, 176, 144, 5, 6)
+    """An engine with every knob open tunes on its first mostly-inter steps
+    (27 of them; or inherits an earlier engine's plan); a later engine on
+    the device inherits the plan without trying anything."""
+    fr = synth.clip(0, 176, 144, 5, 8)
     with Engine() as e:
         sid = e.open(176, 144, 8)
-        for i in range(6):
-            e.submit_frame(sid, fr[i])
+        for i in range(32):
+            e.submit_frame(sid, fr[i % 8])
             e.step()
             e.sync()
         w, c, src = e.launch_shape()
-        assert src in (1, 2) and 1 <= w <= 8
+        plan, _ = e.plan()
+        assert src in (1, 2) and 1 <= w <= 8 and plan["tuning"] == 0
     with Engine() as e2:
         assert e2.launch_shape() == (w, c, 2)
+        assert e2.plan()[0] == dict(plan, source=2)
 
 
 def test_three_steps_in_flight_match_oracle(gpu):
