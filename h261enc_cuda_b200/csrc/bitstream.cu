@@ -60,7 +60,7 @@ __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;"
 
 } // namespace
 #include "ratectrl_dev.h"
-#include "vlc_tables.h"
+#include "vlc_coder.h"
 
 namespace h261b {
 namespace {
@@ -77,30 +77,9 @@ struct CodesSmem {
     alignas(16) int8_t blk[VLC_WARPS][4][64];   /* column-major levels of the blocks in flight */
     alignas(16) uint32_t stage[VLC_WARPS][MB_WORDS];
     uint16_t tc[27][16];
-    uint8_t zz_cm[64];                           /* column-major index of the k-th coefficient sent */
 };
 
 __device__ __forceinline__ uint32_t bswap(uint32_t x) { return __byte_perm(x, 0, 0x0123); }
-
-/* OR a code of len <= 32 bits into MSB-first words at bit position pos of
- * a buffer of `words` words; a position outside it is not written and
- * counts as an error */
-__device__ __forceinline__ void put_bits(uint32_t *w, int words, int pos, uint32_t code, int len, int &oob)
-{
-    if (len <= 0)
-        return;
-    if (pos < 0 || pos + len > words * 32) {
-        oob = 1;
-        return;
-    }
-    const int word = pos >> 5, end = (pos & 31) + len;
-    if (end <= 32) {
-        atomicOr(&w[word], code << (32 - end));
-    } else {
-        atomicOr(&w[word], code >> (end - 32));
-        atomicOr(&w[word + 1], code << (64 - end));
-    }
-}
 
 /* the same on a picture in device memory, whose words hold the stream's
  * bytes in order (byte-swapped) */
@@ -215,10 +194,9 @@ __global__ void __launch_bounds__(VLC_THREADS) codes_kernel(const h261b_session_
     __shared__ CodesSmem sm;
     pdl_launch_dependents();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int i = tid; i < 27 * 16; i += VLC_THREADS)
-        (&sm.tc[0][0])[i] = (&c_vlc_tcoeff[0][0])[i];
-    if (tid < 64)
-        sm.zz_cm[tid] = c_zigzag_cm.cm[tid];
+    load_tcoeff_table(sm.tc, tid, VLC_THREADS);
+    uint32_t zz0, zz1;
+    zigzag_lane(lane, zz0, zz1);
     uint32_t *stage = sm.stage[warp];
     for (int i = lane; i < MB_WORDS; i += 32)
         stage[i] = 0u;
@@ -261,98 +239,13 @@ __global__ void __launch_bounds__(VLC_THREADS) codes_kernel(const h261b_session_
                 *reinterpret_cast<uint2 *>(&sm.blk[warp][slot][j * 8]) =
                     *reinterpret_cast<const uint2 *>(lv + b * 64 + j * 8);
             __syncwarp();
-            int c[8];
-            uint32_t m8 = 0;
-#pragma unroll
-            for (int i = 0; i < 8; i++) {
-                const int8_t x = sm.blk[warp][slot][sm.zz_cm[8 * j + i]];
-                c[i] = (intra && j == 0 && i == 0) ? (int)(uint8_t)x : (int)x;
-                m8 |= (here && c[i] != 0) ? (1u << i) : 0u;
-            }
-            /* the block's nonzero mask in transmission order */
-            uint32_t mlo = j < 4 ? m8 << (8 * j) : 0u, mhi = j >= 4 ? m8 << (8 * (j - 4)) : 0u;
-#pragma unroll
-            for (int o = 1; o < 8; o <<= 1) {
-                mlo |= __shfl_xor_sync(FULL, mlo, o);
-                mhi |= __shfl_xor_sync(FULL, mhi, o);
-            }
-            const uint64_t mask = ((uint64_t)mhi << 32) | mlo;
-            const uint64_t bl = j ? mask & ((1ull << (8 * j)) - 1ull) : 0ull;
-            int prev = bl ? 63 - __clzll((long long)bl) : -1;
-            uint32_t code[8];
-            int clen[8], mine = 0;
-#pragma unroll
-            for (int i = 0; i < 8; i++) {
-                const int k = 8 * j + i;
-                clen[i] = 0;
-                code[i] = 0;
-                if (!((m8 >> i) & 1u))
-                    continue;
-                const int v = c[i];
-                if (k == 0 && intra) {
-                    code[i] = (uint32_t)v & 0xFFu;       /* the DC level as it is */
-                    clen[i] = 8;
-                } else if (k == 0 && (v == 1 || v == -1)) {
-                    code[i] = v < 0 ? 3u : 2u;            /* first inter coefficient +-1 */
-                    clen[i] = 2;
-                } else {
-                    const int run = k - prev - 1;
-                    const int a = v < 0 ? -v : v;
-                    const uint16_t e = (run <= 26 && a <= 15) ? sm.tc[run][a] : (uint16_t)0;
-                    if (e) {
-                        code[i] = ((uint32_t)(e & 0xFF) << 1) | (v < 0 ? 1u : 0u);
-                        clen[i] = (e >> 8) + 1;
-                    } else {
-                        /* escape 0000 01, 6-bit run, 8-bit level */
-                        code[i] = (1u << 14) | ((uint32_t)run << 8) | ((uint32_t)v & 0xFFu);
-                        clen[i] = 20;
-                    }
-                }
-                prev = k;
-                mine += clen[i];
-            }
-            /* offsets of this lane's codes within its block */
-            int incl = mine;
-#pragma unroll
-            for (int o = 1; o < 8; o <<= 1) {
-                const int t = __shfl_up_sync(FULL, incl, o, 8);
-                if (j >= o)
-                    incl += t;
-            }
-            const int last = __shfl_sync(FULL, incl, (slot << 3) | 7);
-            const int btotal = here ? last + 2 : 0;
-            int bstart = pos, rtotal = 0;
-#pragma unroll
-            for (int s2 = 0; s2 < 4; s2++) {
-                const int t = __shfl_sync(FULL, btotal, s2 << 3);
-                if (s2 < slot)
-                    bstart += t;
-                rtotal += t;
-            }
-            if (here) {
-                int p = bstart + incl - mine;
-#pragma unroll
-                for (int i = 0; i < 8; i++) {
-                    put_bits(stage, MB_WORDS, p, code[i], clen[i], oob);
-                    p += clen[i];
-                }
-                if (j == 7)
-                    put_bits(stage, MB_WORDS, bstart + btotal - 2, 2u, 2, oob);   /* EOB */
-            }
-            pos += rtotal;
+            pos += code_block_group(sm.blk[warp][slot], here, intra, zz0, zz1, sm.tc, stage, MB_WORDS, pos, lane,
+                                    oob);
             __syncwarp();
         }
-        oob = __any_sync(FULL, oob);
-        /* store the string and leave the staging words clear for the next */
-        uint32_t *dst = S.vlc_scratch + (size_t)mb * MB_WORDS;
-        const int nw = min((pos + 31) >> 5, MB_WORDS);
-        for (int i = lane; i < nw; i += 32) {
-            dst[i] = stage[i];
-            stage[i] = 0u;
-        }
+        const int bits = store_mb_string(stage, S.vlc_scratch + (size_t)mb * MB_WORDS, pos, oob, lane);
         if (lane == 0)
-            rec.coef_bits = oob ? -1 : pos;   /* -1 makes the layout refuse the picture */
-        __syncwarp();
+            rec.coef_bits = bits;
     }
 }
 
