@@ -1329,9 +1329,19 @@ __global__ void __launch_bounds__(256, KIND == KIND_SEARCH ? H261B_SEARCH_MIN_BL
             if (S.md_in && !(phases & H261B_PHASE_MD))
                 quant += S.md_in[mb].i_quantiser_adjust;
             quant = min(31, max(1, quant)); /* gpu_device.cu:625-627 */
-            uint32_t ssd_l = 0, ssd_c = 0;
-            uint32_t cbp = encdec_pass<FMAD, ABI>(tb, b, S, mb, mbx, mby, m, quant, true, lane, colsum, ssd_l);
-            cbp |= encdec_pass<FMAD, ABI>(tb, b, S, mb, mbx, mby, m, quant, false, lane, colsum, ssd_c);
+            /* the luma pass, then the chroma pass: one copy of the pass's
+             * code run twice (two inlined copies miss the instruction cache
+             * more) */
+            uint32_t ssd_l = 0, ssd_c = 0, cbp = 0;
+#pragma unroll 1
+            for (int pass = 0; pass < 2; pass++) {
+                uint32_t e = 0;
+                cbp |= encdec_pass<FMAD, ABI>(tb, b, S, mb, mbx, mby, m, quant, pass == 0, lane, colsum, e);
+                if (pass == 0)
+                    ssd_l = e;
+                else
+                    ssd_c = e;
+            }
             if (S.ssd_out) {
                 const uint32_t ey = __reduce_add_sync(FULL, ssd_l);
                 const uint32_t ecb = __reduce_add_sync(FULL, lane < 8 ? ssd_c : 0u);
