@@ -9,8 +9,9 @@
  *
  * Three launches; the macroblock-parallel ones take contiguous ranges of the
  * step's work list, one warp per macroblock, so that every SM takes part
- * whatever the mix of picture sizes, and kernel boundaries order the
- * phases (nothing waits on a flag):
+ * whatever the mix of picture sizes.  Kernel boundaries order layout and
+ * pack; codes starts on a picture as soon as the encode launch has counted
+ * all of its MBs done:
  *
  *   codes   the macroblock's coded blocks, four at a time with eight lanes
  *           per block (lane j holds positions 8j..8j+7 of the transmission
@@ -33,9 +34,14 @@
  *
  * All three are programmatic dependent launches: the kernel before each
  * one (the encode kernel, codes, layout) lets it launch as soon as its own
- * CTAs are running, and its CTAs wait (griddepcontrol.wait) for the whole
- * previous grid and its memory before they read what it wrote, so each
- * launch's latency overlaps the kernel before it.  The events that mark the
+ * CTAs are running, so each launch's latency overlaps the kernel before it.
+ * Layout and pack wait (griddepcontrol.wait) for the whole previous grid
+ * and its memory before they read what it wrote.  Codes instead waits per
+ * picture, bounded, on the count the encode warps release after their
+ * writes (session_dev_t.mbs_done), so that it codes the pictures finished
+ * early while the encode launch's last MBs still run on other SMs; it
+ * starts only once every encode CTA is running, and no encode CTA waits on
+ * it.  The events that mark the
  * encode kernel's end are recorded on a side stream, so that nothing sits
  * between the encode kernel and codes in the stream.
  */
@@ -182,14 +188,42 @@ __device__ __forceinline__ void warp_range(int32_t n_work, int &lo, int &hi)
     hi = min(lo + chunk, n_work);
 }
 
+/* Waits (lane 0) until an encoding launch has finished every MB of a
+ * picture: an acquire load of the count the encode warps add to after
+ * fencing their levels and records.  The codes kernel is a programmatic
+ * dependent of that launch, so it starts once every encode CTA is running,
+ * and no encode CTA waits on it: the count completes.  The wait is bounded
+ * all the same (bound_ns of globaltimer, or 2^22 polls); false when it
+ * gives up. */
+__device__ __forceinline__ bool wait_picture_encoded(const int32_t *done, int32_t nmb, uint64_t bound_ns)
+{
+    uint64_t t0 = 0;
+    for (int it = 0; it < (1 << 22); it++) {
+        int32_t v;
+        asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(done) : "memory");
+        if (v >= nmb)
+            return true;
+        uint64_t t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (it == 0)
+            t0 = t;
+        else if (t - t0 > bound_ns)
+            return false;
+        __nanosleep(200);
+    }
+    return false;
+}
+
 /* work items a codes warp takes per draw: an intra MB codes six blocks, a
  * skipped inter MB none, so a static split leaves SMs idle at the end */
 constexpr int CODES_DRAW = 2;
 
 /* ---- codes: each macroblock's coefficient bit string */
+/* extra > 0 (the checking build's test of the bounded wait): wait for
+ * that many MBs more than a picture has, for 2 ms at most */
 __global__ void __launch_bounds__(VLC_THREADS) codes_kernel(const h261b_session_dev_t *sessions,
                                                             const uint32_t *work, int32_t n_work,
-                                                            h261b_step_dev_t *step)
+                                                            h261b_step_dev_t *step, int32_t extra)
 {
     __shared__ CodesSmem sm;
     pdl_launch_dependents();
@@ -200,13 +234,16 @@ __global__ void __launch_bounds__(VLC_THREADS) codes_kernel(const h261b_session_
     uint32_t *stage = sm.stage[warp];
     for (int i = lane; i < MB_WORDS; i += 32)
         stage[i] = 0u;
-    pdl_wait();   /* the encode kernel's records and levels */
+    /* no wait for the whole encode grid: each picture is coded once its
+     * MBs are (the encode launch's tail overlaps this kernel) */
     __syncthreads();
 
     const int slot = lane >> 3, j = lane & 7;
     /* the warp draws CODES_DRAW items at a time from the step's counter
      * (zeroed by the step's descriptor upload) until the list is done */
     int lo = 0, hi = 0;
+    int ready = -1;         /* the last session seen complete             */
+    bool failed = false;    /* a wait gave up: code nothing more          */
     for (int w = 0;; w++) {
         if (w >= hi) {
             int d = 0;
@@ -219,9 +256,24 @@ __global__ void __launch_bounds__(VLC_THREADS) codes_kernel(const h261b_session_
             w = lo;
         }
         const uint32_t item = work[w];
-        const h261b_session_dev_t &S = sessions[item >> 12];
-        if (!S.bits_out)
+        const int sidx = (int)(item >> 12);
+        const h261b_session_dev_t &S = sessions[sidx];
+        if (!S.bits_out || failed)
             continue;
+        if (sidx != ready) {
+            int ok = 0;
+            if (lane == 0)
+                ok = wait_picture_encoded(&S.mbs_done, S.mbw * S.mbh + extra,
+                                          extra ? 2000000ull : 200000000ull) ? 1 : 0;
+            __syncwarp();   /* orders lane 0's acquire before every lane's reads */
+            if (!__shfl_sync(FULL, ok, 0)) {
+                if (lane == 0)
+                    atomicExch(&step->codes_failed, 1u);
+                failed = true;
+                continue;
+            }
+            ready = sidx;
+        }
         const int mb = (int)(item & 4095u);
         h261b_mb_info_t &rec = S.info_out[mb];
         const int cbp = coded_blocks(rec);
@@ -272,7 +324,7 @@ __global__ void __launch_bounds__(LAYOUT_THREADS) layout_kernel(const h261b_sess
     const int gq = S.rc ? S.rc->picture_quant : S.quant;
     const h261b_mb_info_t *info = S.info_out;
     if (tid == 0)
-        bad = 0;
+        bad = step->codes_failed ? 1 : 0;   /* some picture's strings are missing */
     __syncthreads();
 
     const int nwarps = blockDim.x >> 5;
@@ -618,7 +670,8 @@ static cudaError_t launch_dependent(void (*kernel)(Params...), dim3 grid, dim3 b
 
 extern "C" int h261b_launch_bitstream(h261b_session_dev_t *sessions_dev, int32_t n_sessions, const uint32_t *work_dev,
                                       int32_t n_work, h261b_step_dev_t *step, uint8_t *host_arena_dev,
-                                      int64_t host_cap, int32_t sm_count, void *stream, void *layout_done_event)
+                                      int64_t host_cap, int32_t sm_count, void *stream, void *layout_done_event,
+                                      int32_t test_extra_wait)
 {
     if (n_work <= 0 || n_sessions <= 0)
         return 0;
@@ -634,7 +687,7 @@ extern "C" int h261b_launch_bitstream(h261b_session_dev_t *sessions_dev, int32_t
     const int ctas = (int)std::min<int64_t>(want, (int64_t)sm_count * pack_res);
     cudaStream_t st = (cudaStream_t)stream;
     err = launch_dependent(codes_kernel, dim3(codes_ctas), dim3(VLC_THREADS), st,
-                           (const h261b_session_dev_t *)sessions_dev, work_dev, n_work, step);
+                           (const h261b_session_dev_t *)sessions_dev, work_dev, n_work, step, test_extra_wait);
     if (err != cudaSuccess)
         return (int)err;
     err = launch_dependent(layout_kernel, dim3(n_sessions), dim3(LAYOUT_THREADS), st,

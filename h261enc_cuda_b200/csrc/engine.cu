@@ -368,6 +368,7 @@ struct h261b_engine_s {
 
     /* phases-word bits the checking build adds for its tests (0 otherwise) */
     int32_t test_bits = 0;
+    int32_t test_codes_extra = 0;   /* checking build: the codes wait's test */
     /* the encode kernel's launch plan, and its tuning */
     LaunchPlan plan;
     Tuner tuner;
@@ -653,6 +654,9 @@ extern "C" int h261b_engine_create(const h261b_engine_config_t *cfg, h261b_engin
      * first bulk staging announces more bytes than it copies */
     if (getenv("H261B_TEST_STAGE_SHORT"))
         e->test_bits |= H261B_STAGE_SHORT;
+    /* and of the codes kernel's bounded wait for a picture's MBs */
+    if (getenv("H261B_TEST_CODES_WAIT"))
+        e->test_codes_extra = 1;
 #endif
     *out = e;
     return H261B_OK;
@@ -1419,15 +1423,18 @@ extern "C" int h261b_engine_step(h261b_engine_t *e)
         if (n_bits) {
             lr = h261b_launch_bitstream(desc_dev, (int32_t)n, work_dev, n_work, (h261b_step_dev_t *)dm.dev,
                                         e->bits[p].dev, (int64_t)e->bits[p].cap, e->sm_count, st,
-                                        n_rc ? (void *)e->layout_done[p] : nullptr);
+                                        n_rc ? (void *)e->layout_done[p] : nullptr, e->test_codes_extra);
             if (lr != 0) {
                 set_error("bitstream launch failed: %s", cudaGetErrorString((cudaError_t)lr));
                 return H261B_ERR_CUDA;
             }
             H261B_CUDA_TRY(cudaEventRecordWithFlags(e->b_end[p], st, rf));
         }
-        H261B_CUDA_TRY(cudaMemcpyAsync(rm.host, rm.dev, d2h, cudaMemcpyDeviceToHost, st));
+        /* the records download waits for the encode kernel's end: the
+         * bitstream kernels may finish first (the codes kernel waits only
+         * for the pictures that write a bitstream) */
         H261B_CUDA_TRY(cudaStreamWaitEvent(st, e->join_ev[p], 0));
+        H261B_CUDA_TRY(cudaMemcpyAsync(rm.host, rm.dev, d2h, cudaMemcpyDeviceToHost, st));
         H261B_CUDA_TRY(cudaEventRecordWithFlags(e->t_end[p], st, rf));
         H261B_CUDA_TRY(cudaEventRecordWithFlags(e->step_done[p], st, rf));
         return H261B_OK;

@@ -80,7 +80,10 @@ typedef struct {
 typedef struct {
     uint32_t host_used;       /* bytes of the host arena handed out          */
     uint32_t codes_next;      /* work items the codes kernel has handed out  */
-    uint32_t pad[62];
+    uint32_t codes_failed;    /* nonzero: a codes warp gave up waiting for a
+                                 picture's MBs (the layout refuses every
+                                 picture of the step)                        */
+    uint32_t pad[61];
 } h261b_step_dev_t;
 
 typedef struct {
@@ -125,6 +128,12 @@ typedef struct {
     /* sums of squared errors of the picture's Y, Cb, Cr reconstruction
      * (sessions that measure PSNR), zeroed before the step */
     unsigned long long *ssd_out;
+    /* MBs of the picture an encoding launch has finished, zero before the
+     * step: each warp adds a run's MBs after a fence, so that the codes
+     * kernel (a programmatic dependent of the encode launch) may code a
+     * picture as soon as its count is complete, while the encode launch
+     * still works on other pictures */
+    int32_t mbs_done;
 } h261b_session_dev_t;
 
 /* coefficient bits of one MB at most: six blocks of an 8-bit DC or a first
@@ -183,10 +192,13 @@ int h261b_launch_ratectrl(h261b_session_dev_t *sessions_dev, int32_t n_sessions,
  * launches (coefficient codes and packing over the step's work list, the
  * layout per session; the CTA that packs a picture's last MBs copies it);
  * the picture ends in bits_out and in the host arena (device-mapped pinned
- * memory, host_cap bytes) at an offset drawn from step->host_used */
+ * memory, host_cap bytes) at an offset drawn from step->host_used.
+ * test_extra_wait > 0 (tests of the checking build only): the codes kernel
+ * waits for that many MBs more than each picture has, for 2 ms, so that its
+ * bounded wait runs out and the step's pictures are refused */
 int h261b_launch_bitstream(h261b_session_dev_t *sessions_dev, int32_t n_sessions, const uint32_t *work_dev,
                            int32_t n_work, h261b_step_dev_t *step, uint8_t *host_arena_dev, int64_t host_cap,
-                           int32_t sm_count, void *stream, void *layout_done_event);
+                           int32_t sm_count, void *stream, void *layout_done_event, int32_t test_extra_wait);
 /* device bytes per step slot a w x h session's bitstream needs: picture
  * bytes, MB scratch and offsets (0: no bitstream for this size), and where
  * each part starts in that block */

@@ -1076,8 +1076,12 @@ __device__ __forceinline__ void publish_run(const h261b_session_dev_t &S, int t,
     __threadfence();
     __syncwarp();
     uint32_t last = 0;
-    if (lane == 0)
+    if (lane == 0) {
         last = atomicAdd(&dn->ticket, (uint32_t)n) + (uint32_t)n == (uint32_t)(S.mbw * S.mbh) ? 1u : 0u;
+        /* the run's levels and records are written and fenced: count its
+         * MBs for the codes kernel */
+        atomicAdd(const_cast<int32_t *>(&S.mbs_done), n);
+    }
     last = __shfl_sync(FULL, last, 0);
     if (last) {
         __threadfence();

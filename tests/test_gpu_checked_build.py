@@ -125,3 +125,59 @@ def test_bounded_staging_wait_runs_out_and_reports(gpu):
     assert res["forced_timeouts"] > 0, res
     assert res["forced_ok"], "the output changed when the staging wait ran out"
     assert res["normal_timeouts"] == 0 and res["normal_ok"], res
+
+
+CODES_WAIT_CHILD = r'''
+import json, os, sys
+import numpy as np
+sys.path.insert(0, ROOT); sys.path.insert(0, ROOT + "/oracle")
+import oracle as O
+from h261enc_cuda_b200 import synth
+from h261enc_cuda_b200.engine import Engine
+w, h, n = 176, 144, 3
+fr = synth.clip(2, w, h, 83, n)
+want = O.encode_sequence(fr, w, h, 8)
+
+def encode():
+    out = []
+    with Engine(warps_per_cta=4, kernel_split=1, tail_items=3, staging=1, levels_to_host=1) as e:
+        sid = e.open(w, h, 8, bitstream=1)
+        for i in range(n):
+            e.submit_frame(sid, fr[i])
+            e.step()
+            e.sync()
+            r = e.result(sid)
+            same = (np.array_equal(r.to_abi(w)["tcoeff"], want["mbs"][i]["tcoeff"]) and
+                    np.array_equal(np.concatenate(e.recon(sid)), want["recon"][i]))
+            wrote = O.write_picture_oracle(r.to_abi(w), w, h, i, r.frame_type, 8)
+            out.append({"status": int(r.bits_status), "same": bool(same),
+                        "bits_ok": r.bits is not None and r.bits == wrote})
+    return out
+
+forced = encode()                       # every codes warp's wait runs out
+del os.environ["H261B_TEST_CODES_WAIT"]
+normal = encode()                       # a new engine in the same context
+print(json.dumps({"forced": forced, "normal": normal}))
+'''
+
+
+@pytest.mark.gpu
+def test_bounded_codes_wait_runs_out_and_refuses(gpu):
+    """The codes kernel waits, bounded, for each picture's MBs to be counted
+    done by the encode launch.  The checking build can make it wait for one
+    MB more than the picture has (H261B_TEST_CODES_WAIT), for 2 ms: the wait
+    runs out, the step is marked and the layout refuses its pictures (a
+    negative bitstream status), while the records and reconstructions are
+    still the oracle's; a new engine in the same process then writes every
+    picture's bitstream as the oracle's writer does.  No fault and no hang
+    is made; the failure is a count that never completes."""
+    lib = os.path.join(ROOT, "h261enc_cuda_b200", "lib", "libh261b_check.so")
+    if not os.path.exists(lib):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "h261enc_cuda_b200", "csrc"), "check"], check=True)
+    env = dict(os.environ, H261B_LIB="check", H261B_TEST_CODES_WAIT="1")
+    r = subprocess.run([sys.executable, "-c", f"ROOT = {ROOT!r}\n" + CODES_WAIT_CHILD], env=env,
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    res = json.loads(r.stdout.strip().splitlines()[-1])
+    assert all(p["status"] < 0 and p["same"] for p in res["forced"]), res
+    assert all(p["status"] == 0 and p["same"] and p["bits_ok"] for p in res["normal"]), res
