@@ -414,20 +414,33 @@ class Runner:
         self.dev = [np.array([[pl[i][c] for i in range(len(pl))] for pl in (p[2] for p in pools)], np.uint64)
                     for c in range(3)]
         self.rows = np.arange(len(streams))
+        # per-step arrays rewritten in place (the submission takes their
+        # addresses): plane offsets, clip positions, plane addresses
+        n = len(streams)
+        self.cb_off = self.ny.copy()
+        self.cr_off = self.ny + self.ny // 4
+        self.pmod = np.zeros(n, np.int64)
+        self.idx = np.zeros(n, np.uint64)
+        self.y, self.cb, self.cr = (np.zeros(n, np.uint64) for _ in range(3))
+        self.ptrs = (self.sids.ctypes.data, self.y.ctypes.data, self.cb.ctypes.data, self.cr.ctypes.data)
+        self.until = 0             # steps before some stream may need a restart
 
     def _advance(self):
         """The clip picture each stream sends next (array ops: the call sits
         on the host's per-step path)."""
-        if (self.pos >= self.length).any():
+        if self.until <= 0:
             for k in np.flatnonzero(self.pos >= self.length):
                 s = self.streams[k]
                 self.ending.append((int(self.sids[k]), self.queued - 1))
                 self.sids[k] = self.e.open(s.width, s.height, s.quant, bitstream=1)
                 self.pos[k] = 0
-        idx = self.index[self.pos % self.period]
+            self.until = int((self.length - self.pos).min())
+        np.remainder(self.pos, self.period, out=self.pmod)
+        np.take(self.index, self.pmod, out=self.idx)
         self.pos += 1
+        self.until -= 1
         self.queued += 1
-        return idx
+        return self.idx
 
     def retire(self, read_step):
         """Close the streams whose last picture was in a step already read."""
@@ -448,8 +461,11 @@ class Runner:
         """The next picture of every stream from host memory, in one call
         (wait=False: the copies run while the caller goes on)."""
         idx = self._advance()
-        y = self.base + idx * self.fbytes
-        self.e.submit_batch(self.sids, y, y + self.ny, y + self.ny + self.ny // 4, wait=wait)
+        np.multiply(idx, self.fbytes, out=self.y)
+        np.add(self.y, self.base, out=self.y)
+        np.add(self.y, self.cb_off, out=self.cb)
+        np.add(self.y, self.cr_off, out=self.cr)
+        self.e.submit_batch_ptrs(len(self.streams), *self.ptrs, wait=wait)
 
 
 def ours(args, world, rank, local, dist):

@@ -162,6 +162,15 @@ class Engine:
         check(fn(self._h, sids.size, sids.ctypes.data, ptrs[0].ctypes.data, ptrs[1].ctypes.data,
                  ptrs[2].ctypes.data, None if q is None else q.ctypes.data), "h261b_engine_submit_batch")
 
+    def submit_batch_ptrs(self, n: int, sids_ptr: int, y_ptr: int, cb_ptr: int, cr_ptr: int,
+                          quants_ptr: int = 0, wait: bool = True) -> None:
+        """``submit_batch`` with the addresses of the caller's own arrays
+        (n int32 session ids, n uint64 plane addresses each, optionally n
+        int32 QUANTs): no conversion on the per-step path, for a caller that
+        keeps those arrays and rewrites them in place every step."""
+        fn = _lib.core().h261b_engine_submit_batch if wait else _lib.core().h261b_engine_submit_batch_async
+        check(fn(self._h, n, sids_ptr, y_ptr, cb_ptr, cr_ptr, quants_ptr or None), "h261b_engine_submit_batch")
+
     def submit_frames(self, sids, frames, quants=None, wait: bool = True) -> None:
         """``submit_batch`` for packed frames (uint8 arrays of W*H*3/2)."""
         y = np.array([f.ctypes.data for f in frames], np.uint64)

@@ -3,6 +3,8 @@ every stream plays its clip forwards and backwards, a stream that reaches
 its length is replaced by a new session and its old one is closed only once
 the step holding its last picture has been read, and the device-picture
 batch names each stream's current picture."""
+import ctypes
+
 import numpy as np
 
 import bench
@@ -22,6 +24,11 @@ class _Engine:
 
     def submit_device_batch(self, sids, y, cb, cr):
         self.device_batch = (np.array(sids), np.array(y), np.array(cb), np.array(cr))
+
+    def submit_batch_ptrs(self, n, sids_ptr, y_ptr, cb_ptr, cr_ptr, quants_ptr=0, wait=True):
+        arr = lambda p, t: np.ctypeslib.as_array((t * n).from_address(p)).copy()
+        self.host_batch = (arr(sids_ptr, ctypes.c_int32), arr(y_ptr, ctypes.c_uint64), arr(cb_ptr, ctypes.c_uint64),
+                           arr(cr_ptr, ctypes.c_uint64))
 
 
 class _Stream:
@@ -67,3 +74,26 @@ def test_runner_advances_restarts_and_retires():
     assert first_sids[0] in e.closed
     for sid, last in run.ending:
         assert last > 240 - 3 and sid not in e.closed
+
+
+def test_runner_host_batch_addresses():
+    """The host-picture batch, written in place into arrays whose addresses
+    the submission takes: each stream's current clip picture and its planes,
+    across restarts."""
+    lengths = [30, 47, 100]
+    streams = [_Stream(n) for n in lengths]
+    e = _Engine()
+    pools = _pools(len(streams), bench.CLIP_LEN)
+    run = bench.Runner(e, streams, pools)
+    pos = [0] * len(streams)
+    for step in range(240):
+        run.queue_host(wait=False)
+        sids, y, cb, cr = e.host_batch
+        assert list(sids) == list(run.sids)
+        for k, s in enumerate(streams):
+            if pos[k] >= s.length:
+                pos[k] = 0
+            i = workloads.clip_index(pos[k], bench.CLIP_LEN)
+            pos[k] += 1
+            base = pools[k][1].ctypes.data + i * pools[k][1].shape[1]
+            assert y[k] == base and cb[k] == base + 176 * 144 and cr[k] == base + 176 * 144 * 5 // 4, (step, k)
